@@ -1,0 +1,390 @@
+"""Benchmark of the CSR x dense SpMM forward on B200.
+
+Workload (one step): the plain FP16 forward of G independent copies of the
+sweep matrix 4096 x 1024 at 80% sparsity (Zipf(1.2) row lengths, values
+N(0, 0.03)), B 1024 x 256 FP16 U(-1, 1), FP16 output with FP32 accumulation.
+Four seeded patterns are each replicated G/4 times into separate device
+buffers, so that the inputs of one step (G = 32: ~245 MB) exceed the 126 MB
+L2 and every problem is read from HBM.
+
+  value      GFLOP/s (2 nnz N per problem) with inputs resident in HBM,
+             device time of K steps (CUDA events), max over ranks
+  e2e        the same metric through the host-buffer entry point
+             (tca_spmm_host, the reference's calling convention): per step one
+             problem's CSR and B are copied in from pinned memory, the plan is
+             built, the forward runs and C is copied back
+  roofline   HBM roofline of the dominant kernel: algorithmic bytes of the
+             work it does per launch / its mean CUDA-event duration
+  cpu_baseline  the oracle's OpenMP FP32 CSR x dense on the host cores, one
+             problem, repeated for a bounded time
+
+--impl reference runs the reference's own TCA kernel (our_spmm_balanced,
+built from the reference sources into oracle/_ref) through its host API on
+the same problems, plus the reference's cuSPARSE comparator.
+
+Multi-GPU (torchrun): each rank runs its own G problems (row-independent
+work, no collective on the data path): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "tca-spmm_b200" / "python"))
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SpMM GFLOP/s (2*nnz*N), FP16 in, FP32 accumulate, FP16 out"
+WORKLOAD = "sweep 4096x1024 sparsity 0.80 zipf(1.2) N=256"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--problems", type=int, default=32, help="independent problems per step")
+    ap.add_argument("--sparsity", type=float, default=0.80)
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons with NVML while running."""
+
+    def __init__(self, device_index=0, period=0.01):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._period = period
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # NVML missing: report it, do not guess
+            self._nv = None
+            self.error = str(e)
+
+    def _run(self):
+        nv = self._nv
+        names = {
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+            "hw_power_brake_slowdown": getattr(nv, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80),
+        }
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for k, bit in names.items():
+                    if mask & bit:
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            time.sleep(self._period)
+
+    def __enter__(self):
+        if self._nv is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._nv is not None:
+            self._t.join()
+
+    def summary(self):
+        if self._nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "note": "NVML unavailable"}
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_problems(args):
+    from tca_spmm import gen
+    distinct = [gen.sweep(args.sparsity, N=args.n, seed=7000 + i) for i in range(4)]
+    return distinct
+
+
+def problem_bytes(c, N, c_bytes=2):
+    nnz = int(c["col"].size)
+    return nnz * (2 + 4) + (c["M"] + 1) * 4 + c["K"] * N * 2 + c["M"] * N * c_bytes
+
+
+def cpu_baseline(c, seconds):
+    from oracle import oracle
+    nthreads = len(os.sched_getaffinity(0))
+    flops = 2.0 * c["col"].size * c["B"].shape[1]
+    oracle.spmm_f32(c["row_ptr"], c["col"], c["vals"], c["B"], nthreads=nthreads)  # warm-up
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        oracle.spmm_f32(c["row_ptr"], c["col"], c["vals"], c["B"], nthreads=nthreads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or reps >= 1000:
+            break
+    return {"value": round(flops * reps / el / 1e9, 3), "unit": "GFLOP/s", "cores": nthreads, "kind": "port",
+            "sample": f"{reps} runs of one {c['M']}x{c['K']} problem (nnz={c['col'].size}, N={c['B'].shape[1]}) "
+                      f"in {el:.1f} s, OpenMP FP32 CSR x dense (oracle/tca_oracle.c orc_spmm_f32)"}
+
+
+def dist_setup(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(x, world):
+    import torch
+    import torch.distributed as dist
+    if world == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args, world, rank):
+    import torch
+    import tca_spmm
+    distinct = make_problems(args)
+    G = args.problems
+    dev = torch.device("cuda", torch.cuda.current_device())
+    probs = []
+    for g in range(G):
+        c = distinct[g % len(distinct)]
+        rp = torch.from_numpy(c["row_ptr"]).to(dev)
+        ci = torch.from_numpy(c["col"]).to(dev)
+        v = torch.from_numpy(c["vals"]).to(dev)
+        B = torch.from_numpy(c["B"]).to(dev)
+        C = torch.empty((c["M"], args.n), dtype=torch.float16, device=dev)
+        plan = tca_spmm.Plan(rp, ci, v, c["K"])
+        probs.append((c, plan, B, C))
+    torch.cuda.synchronize()
+    info = probs[0][1].info()
+    flops_step = sum(2.0 * c["col"].size * args.n for c, *_ in probs)
+    bytes_step = sum(problem_bytes(c, args.n) for c, *_ in probs)
+    in_bytes_step = sum(problem_bytes(c, args.n) - c["M"] * args.n * 2 for c, *_ in probs)
+    plans = [p for _, p, _, _ in probs]
+    Bs = [B for _, _, B, _ in probs]
+    Cs = [C for _, _, _, C in probs]
+    # one batched call per step: tensor-core launches (<= 32 problems each, one
+    # N-slice width here) then CUDA-core launches (<= 32 problems each)
+    n_tc_jobs = sum(1 for p in plans if p.info()["n_tc_windows"] > 0)
+    n_cc_jobs = sum(1 for p in plans if p.info()["n_cc_windows"] > 0)
+    launches_per_step = -(-n_tc_jobs // 32) + -(-n_cc_jobs // 32)
+
+    def step():
+        tca_spmm.spmm_batched(plans, Bs, Cs)
+
+    for _ in range(args.warmup):
+        step()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier(world)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        barrier(world)
+    ms_total = max_over_ranks(e0.elapsed_time(e1), world)
+    ms_step = ms_total / args.steps
+    value = world * flops_step / (ms_step * 1e-3) / 1e9
+
+    # per-kernel device time: a second pass over the same steps with CUDA
+    # events recorded around the tensor-core and the CUDA-core launches
+    n_prof = max(1, min(args.steps, 20))
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(n_prof)]
+    for e4 in evs:
+        for e in e4:
+            e.record()
+    torch.cuda.synchronize()
+    for k in range(n_prof):
+        tca_spmm.spmm_batched(plans, Bs, Cs, events=evs[k])
+    torch.cuda.synchronize()
+    tc_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    cc_ms = [e[2].elapsed_time(e[3]) for e in evs]
+    # algorithmic bytes per launch, per problem part: the part's nonzeros
+    # (2 B value + 4 B index), row offsets and output rows, plus B once
+    tc_bytes = cc_bytes = 0
+    for p in plans:
+        inf = p.info()
+        tc_rows = min(inf["M"], inf["n_tc_windows"] * 128)
+        cc_rows = inf["M"] - tc_rows
+        if inf["n_tc_windows"]:
+            tc_bytes += inf["tc_nnz"] * 6 + (tc_rows + 1) * 4 + inf["K"] * args.n * 2 + tc_rows * args.n * 2
+        if inf["n_cc_windows"]:
+            cc_bytes += ((inf["nnz"] - inf["tc_nnz"]) * 6 + (cc_rows + 1) * 4 + inf["K"] * args.n * 2
+                         + cc_rows * args.n * 2)
+    tc_mean, cc_mean = float(np.mean(tc_ms)), float(np.mean(cc_ms))
+    dominant = "spmm_tc_kernel" if n_tc_jobs and tc_mean >= cc_mean else "spmm_cc_rows_kernel"
+    dom_ms, dom_bytes = (tc_mean, tc_bytes) if dominant == "spmm_tc_kernel" else (cc_mean, cc_bytes)
+    peak, peak_kind = peaks()
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(dominant)
+
+    # e2e through the host-buffer entry point
+    e2e_steps = max(1, min(args.steps, 8))
+    pinned = []
+    for c in distinct:
+        pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+        pinned.append(dict(rp=pin(c["row_ptr"]), ci=pin(c["col"]), v=pin(c["vals"]), B=pin(np.ascontiguousarray(c["B"])),
+                           C=torch.empty((c["M"], args.n), dtype=torch.float16).pin_memory().numpy(), c=c))
+    tca_spmm.spmm_host(pinned[0]["rp"], pinned[0]["ci"], pinned[0]["v"], 1024, pinned[0]["B"], C=pinned[0]["C"],
+                       keep_empty_rows=False)
+    barrier(world)
+    t0 = time.perf_counter()
+    e2e_flops = 0.0
+    h2d = d2h = 0
+    for s in range(e2e_steps):
+        p = pinned[s % len(pinned)]
+        tca_spmm.spmm_host(p["rp"], p["ci"], p["v"], p["c"]["K"], p["B"], C=p["C"], keep_empty_rows=False)
+        e2e_flops += 2.0 * p["c"]["col"].size * args.n
+        h2d += p["rp"].nbytes + p["ci"].nbytes + p["v"].nbytes + p["B"].nbytes
+        d2h += p["C"].nbytes
+    barrier(world)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = {"value": round(world * e2e_flops / e2e_s / 1e9, 3), "unit": "GFLOP/s",
+           "h2d_bytes_per_step": h2d // e2e_steps, "d2h_bytes_per_step": d2h // e2e_steps,
+           "steps": e2e_steps, "path": "tca_spmm_host (host buffers, plan build inside the timed region)"}
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
+        "data": "synthetic (seeded numpy PCG64)",
+        "config": {"workload": WORKLOAD, "problems_per_step": G, "distinct_patterns": len(distinct),
+                   "M": 4096, "K": 1024, "N": args.n, "sparsity": args.sparsity,
+                   "nnz_per_problem": [int(c["col"].size) for c in distinct],
+                   "bytes_per_step": bytes_step, "input_bytes_per_step": in_bytes_step,
+                   "l2": "inputs larger than L2 (126 MB): each problem's buffers are distinct",
+                   "parallelism": f"dp{world} (independent problems per rank)",
+                   "plan": info},
+        "hbm_gbs_achieved_step": round(world * bytes_step / (ms_step * 1e-3) / 1e9, 1),
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                     "mean_launch_us": round(dom_ms * 1e3, 3),
+                     "kernels_us": {"spmm_tc_kernel": round(tc_mean * 1e3, 3),
+                                    "spmm_cc_rows_kernel": round(cc_mean * 1e3, 3)}},
+        "e2e": e2e,
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk.summary(),
+    }
+    return out, distinct
+
+
+def run_reference(args, world, rank):
+    import torch
+    from oracle import oracle
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libtcaref.so was not built (reference tree absent at build time)"}, None
+    distinct = make_problems(args)
+    n_iter = max(1, args.steps)
+    ms_kernel, flops, wall = [], 0.0, 0.0
+    sp_ms = []
+    with oracle.quiet_stdout():
+        oracle.ref_our_spmm_balanced(distinct[0]["row_ptr"], distinct[0]["col"], distinct[0]["vals"], 1024,
+                                     distinct[0]["B"], n_iter=1)
+        for c in distinct:
+            t0 = time.perf_counter()
+            _, ms = oracle.ref_our_spmm_balanced(c["row_ptr"], c["col"], c["vals"], c["K"], c["B"], n_iter=1)
+            wall += time.perf_counter() - t0
+            _, ms = oracle.ref_our_spmm_balanced(c["row_ptr"], c["col"], c["vals"], c["K"], c["B"], n_iter=n_iter)
+            ms_kernel.append(ms)
+            flops += 2.0 * c["col"].size * args.n
+            A = oracle.csr_to_dense(c["M"], c["K"], c["row_ptr"], c["col"], c["vals"])
+            _, ms_sp = oracle.ref_cusparse_spmm(A, c["B"], n_iter=n_iter)
+            sp_ms.append(ms_sp)
+    value = flops / (sum(ms_kernel) * 1e-3) / 1e9
+    e2e = flops / wall / 1e9
+    h2d = sum(c["row_ptr"].nbytes + c["col"].nbytes + c["vals"].nbytes + c["B"].nbytes + c["M"] * args.n * 4
+              for c in distinct) // len(distinct)
+    d2h = distinct[0]["M"] * args.n * 4
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sum(ms_kernel) / len(ms_kernel), 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
+        "data": "synthetic (seeded numpy PCG64)",
+        "config": {"workload": WORKLOAD, "problems": len(distinct), "N": args.n,
+                   "timing": "the reference's own event timing of n_iter back-to-back launches per call "
+                             "(src/our_spmm.cu:552-574), hot L2; FP32 output"},
+        "reference_impl": "our_spmm_balanced (TCA kernel, mma.sync) from the unmodified reference sources, "
+                          "compiled for sm_100a into oracle/_ref/libtcaref.so; run through its host API",
+        "cpu_baseline": None,
+        "cusparse": {"value": round(flops / (sum(sp_ms) * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+                     "impl": "perform_cuSPARSE_SpMM (reference comparator, cusparseSpMM CSR ALG_DEFAULT)"},
+        "e2e": {"value": round(e2e, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "path": "our_spmm_balanced(n_iter=1), wall clock"},
+    }
+    return out, distinct
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        out, _ = run_reference(args, 1, 0)
+        print(json.dumps(out), flush=True)
+        return
+    out, distinct = run_ours(args, world, rank)
+    if rank == 0:
+        if world == 1 and not args.no_cpu:
+            out["cpu_baseline"] = cpu_baseline(distinct[0], args.cpu_seconds)
+        else:
+            out["cpu_baseline"] = None
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,232 @@
+/*
+ * tca_spmm.h -- C ABI of the B200 (sm_100a) TCA-SpMM library, libtca_spmm.so.
+ *
+ * Computes C = alpha * A * B + beta * C for a CSR sparse A (M x K, FP16 values,
+ * int32 indices, 0-based) and a dense row-major B (K x N, FP16), accumulating
+ * in FP32 and writing C (M x N, row-major) in FP16 or FP32.
+ *
+ * All array arguments named d_* are device pointers; h_* are host pointers.
+ * Every entry point returns a tca_status_t; on failure
+ * tca_last_error_string() describes the error (per host thread).
+ * Streams are CUDA runtime streams (cudaStream_t); NULL is the legacy default
+ * stream. Reference citations are file:line within the reference project.
+ */
+#ifndef TCA_SPMM_H
+#define TCA_SPMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TCA_API __attribute__((visibility("default")))
+#else
+#define TCA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct CUstream_st;
+typedef struct CUstream_st *tca_stream_t; /* identical to cudaStream_t */
+
+typedef enum tca_status {
+    TCA_OK = 0,
+    TCA_ERR_INVALID_ARG = 1, /* bad size, pointer, alignment or option */
+    TCA_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    TCA_ERR_ALLOC = 3,       /* device or host allocation failed */
+    TCA_ERR_UNSUPPORTED = 4, /* valid request this build does not support */
+    TCA_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    TCA_ERR_FORMAT = 6,      /* malformed CSR or matrix file */
+    TCA_ERR_IO = 7           /* file could not be read */
+} tca_status_t;
+
+typedef enum tca_dtype {
+    TCA_DTYPE_F16 = 0,
+    TCA_DTYPE_F32 = 1,
+    TCA_DTYPE_E4M3 = 2
+} tca_dtype_t;
+
+/* Rows of A without nonzeros leave C untouched, as in the reference, whose
+ * kernel never writes them (src/our_spmm.cu:303-305, :366-369). Without the
+ * flag those rows become beta * C. */
+#define TCA_FLAG_KEEP_EMPTY_ROWS 1u
+
+/* ------------------------------------------------------------------ */
+/* Library information and errors                                     */
+/* ------------------------------------------------------------------ */
+TCA_API const char *tca_version(void);
+TCA_API const char *tca_last_error_string(void);
+TCA_API const char *tca_status_string(int status);
+
+/* ------------------------------------------------------------------ */
+/* Plan-free forward on CUDA cores, straight from CSR.
+ * Replaces the device part of our_spmm_balanced (src/our_spmm.cu:472-588,
+ * kernel at :290-346) without the per-call host schedule
+ * (workload_manager, :347-471). N % 8 == 0 with 16-byte aligned B and C rows
+ * takes the vectorised path; any other N or alignment a scalar one.        */
+/* ------------------------------------------------------------------ */
+TCA_API int tca_spmm_csr(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16,
+                 int M, int K, int nnz,
+                 const void *d_B_f16, int ldb, int N,
+                 void *d_C, int ldc, int c_dtype,
+                 float alpha, float beta, unsigned flags, tca_stream_t stream);
+
+/* ------------------------------------------------------------------ */
+/* Plans: the row-window, column-condensed tile format.
+ * tca_plan_create builds it on the GPU from a device CSR (replacing the
+ * reference's per-call host schedule workload_manager, src/our_spmm.cu:347-471):
+ * rows are ordered by nonzero count, grouped into windows of 128 rows, each
+ * window's distinct columns are condensed into 64-wide chunks, and each window
+ * is assigned to the tensor-core path (tcgen05) or the CUDA-core path by its
+ * condensed density. The plan keeps its own device copy of everything it
+ * needs; the caller's CSR may be freed afterwards.                          */
+/* ------------------------------------------------------------------ */
+typedef struct tca_plan *tca_plan_t;
+
+typedef struct tca_plan_opts {
+    int sort_rows;        /* 1 (default): windows over rows sorted by nnz; 0: natural row order */
+    float tc_min_density; /* windows with condensed density >= this use tensor cores (default 0.02) */
+    int path;             /* 0 auto (default), 1 CUDA cores only, 2 tensor cores only */
+    int reserved[5];
+} tca_plan_opts_t;
+
+typedef struct tca_plan_info {
+    int M, K, nnz;
+    int n_windows;          /* windows of 128 rows */
+    int n_tc_windows;       /* windows on the tensor-core path */
+    int n_cc_windows;       /* windows on the CUDA-core path */
+    int n_tc_chunks;        /* 64-column condensed chunks over all tensor-core windows */
+    int n_images;           /* chunks also kept as dense pre-swizzled tiles */
+    long long tc_nnz;       /* nonzeros carried by tensor-core tiles */
+    long long format_bytes; /* device bytes the plan occupies */
+} tca_plan_info_t;
+
+/* Arrays of a plan, for tca_plan_export (element type in brackets). */
+typedef enum tca_plan_array {
+    TCA_ARR_ROW_PERM = 0,     /* [int, M]   sorted position -> caller's row */
+    TCA_ARR_P_ROW_PTR = 1,    /* [int, M+1] CSR offsets in sorted row order */
+    TCA_ARR_P_COL = 2,        /* [int, nnz] columns in sorted row order */
+    TCA_ARR_P_VAL = 3,        /* [fp16, nnz] values in sorted row order */
+    TCA_ARR_SRC = 4,          /* [int, nnz] caller's nonzero index of each entry */
+    TCA_ARR_TC_WINDOWS = 5,   /* [int, n_tc_windows] */
+    TCA_ARR_CC_WINDOWS = 6,   /* [int, n_cc_windows] */
+    TCA_ARR_TILE_FIRST = 7,   /* [int, n_tc_windows+1] first chunk of each tensor-core window */
+    TCA_ARR_WIN_COLS = 8,     /* [int, n_tc_chunks*64] condensed columns, -1 padded */
+    TCA_ARR_TILE_PTR = 9,     /* [int, n_tc_chunks+1] entry offsets per chunk */
+    TCA_ARR_TILE_ENTRIES = 10,/* [uint32, tc_nnz] local_row<<22 | local_col<<16 | fp16 bits */
+    TCA_ARR_TILE_SRC = 11,    /* [int, tc_nnz] index of each entry into TCA_ARR_P_VAL */
+    TCA_ARR_TILE_IMAGE_IDX = 12, /* [int, n_tc_chunks] dense image of each chunk, -1 = none */
+    TCA_ARR_TILE_IMAGES = 13, /* [fp16, n_images*8192] dense 128x64 tiles, 128-byte swizzled K-major */
+    TCA_ARR_CC_ITEMS = 14,    /* [int pairs] CUDA-core items [first, end) of sorted rows, CUDA-core windows */
+    TCA_ARR_ALL_ITEMS = 15    /* [int pairs] the same over all windows */
+} tca_plan_array_t;
+
+TCA_API void tca_plan_opts_default(tca_plan_opts_t *opts);
+TCA_API int tca_plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16,
+                    int M, int K, int nnz, const tca_plan_opts_t *opts,
+                    tca_stream_t stream, tca_plan_t *plan);
+/* Re-gathers new values for the same sparsity pattern into the plan. */
+TCA_API int tca_plan_update_values(tca_plan_t plan, const void *d_vals_f16, tca_stream_t stream);
+TCA_API int tca_plan_info(tca_plan_t plan, tca_plan_info_t *info);
+/* Copies one plan array (tca_plan_array_t) to host memory; *out_bytes gets its
+ * size. With h_dst NULL only the size is returned. Used to check the GPU build
+ * of the format bit for bit against a host build. */
+TCA_API int tca_plan_export(tca_plan_t plan, int which, void *h_dst, size_t capacity_bytes, size_t *out_bytes);
+/* Reads the plan's device status word (synchronises): TCA_ERR_TIMEOUT when a
+ * bounded device-side wait of an earlier launch gave up, else TCA_OK. */
+TCA_API int tca_plan_status(tca_plan_t plan);
+TCA_API int tca_plan_destroy(tca_plan_t plan);
+
+/* Forward with a plan: C = alpha * A * B + beta * C. Launches the
+ * tensor-core kernel over the plan's tensor-core windows and the CUDA-core
+ * kernel over the rest, in that order, on `stream`. N % 8 == 0, ldb % 8 == 0,
+ * ldc * sizeof(C) % 16 == 0 and 16-byte aligned B and C are needed for the
+ * tensor-core kernel; otherwise every window runs on CUDA cores.
+ * Replaces the device work of our_spmm_balanced (src/our_spmm.cu:547-559). */
+TCA_API int tca_spmm(tca_plan_t plan, const void *d_B_f16, int ldb, int N,
+             void *d_C, int ldc, int c_dtype, float alpha, float beta,
+             unsigned flags, tca_stream_t stream);
+/* tca_spmm that also records four caller-created CUDA events (cudaEvent_t,
+ * NULL entries skipped) on `stream`: events[0]/[1] around the tensor-core
+ * kernel, events[2]/[3] around the CUDA-core kernel -- per-kernel device time
+ * for profiling. Same work as tca_spmm. */
+TCA_API int tca_spmm_events(tca_plan_t plan, const void *d_B_f16, int ldb, int N,
+             void *d_C, int ldc, int c_dtype, float alpha, float beta,
+             unsigned flags, tca_stream_t stream, void *const *events);
+/* One forward of a batched launch. n_tile picks the tensor-core N-slice
+ * width (64, 128 or 256; 0 = by N). */
+typedef struct tca_batch_item {
+    tca_plan_t plan;
+    const void *d_B_f16;
+    int ldb, N;
+    void *d_C;
+    int ldc;
+    int n_tile;
+} tca_batch_item_t;
+
+/* Forwards of many plans (layers of different shapes and sparsity) in a
+ * handful of launches: one tensor-core launch per N-slice width over every
+ * item's tensor-core windows, then one CUDA-core launch per row width over
+ * every item's remaining rows (at most 32 items per launch). Same results as
+ * calling tca_spmm per item. events: as in tca_spmm_events (may be NULL).
+ * No device memory is allocated: the work list travels as kernel parameters,
+ * so the call can be captured in a CUDA graph. */
+TCA_API int tca_spmm_batched(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha,
+                             float beta, unsigned flags, tca_stream_t stream, void *const *events);
+/* How many tensor-core and CUDA-core kernel launches one tca_spmm with this
+ * N makes (0 or 1 each). */
+TCA_API int tca_plan_launch_counts(tca_plan_t plan, int N, int *n_tc_launches, int *n_cc_launches);
+
+/* ------------------------------------------------------------------ */
+/* Host-side matrix I/O and format conversion. Arrays returned through
+ * pointer-to-pointer arguments are malloc'd; release them with tca_free.  */
+/* ------------------------------------------------------------------ */
+TCA_API void tca_free(void *p);
+
+/* Parses .smtx text as smtx_input_to_Dense does (src/file_input.cu:135-193):
+ * header "rows, cols, nnz" split on ',', the row_ptr line, then col_idx tokens
+ * over any number of lines. Extension: one further line of nnz decimal values
+ * (the reference's files carry none and it stores 1.0 at every nonzero; its
+ * reader would misparse such a line). *vals_f16 receives those values, or 1.0
+ * everywhere. Malformed text (bad tokens, wrong counts, decreasing row_ptr,
+ * columns outside [0, cols)) gives TCA_ERR_FORMAT instead of the reference's
+ * exception or overrun. */
+TCA_API int tca_smtx_parse(const char *text, size_t len, int *M, int *K, int *nnz,
+                           int **row_ptr, int **col_idx, void **vals_f16);
+TCA_API int tca_smtx_read(const char *path, int *M, int *K, int *nnz,
+                          int **row_ptr, int **col_idx, void **vals_f16);
+/* Writes the smtx layout (values line only when vals_f16 is not NULL). */
+TCA_API int tca_smtx_write(const char *path, int M, int K, int nnz, const int *row_ptr,
+                           const int *col_idx, const void *vals_f16);
+
+/* Dense row-major FP16 -> CSR, as convert_dense_to_csr (src/miscalleneous.cu:29-65):
+ * an element is a nonzero iff its value compares != 0 (so -0.0 is dropped). */
+TCA_API int tca_dense_to_csr(const void *mat_f16, int M, int K, int *nnz,
+                             int **row_ptr, int **col_idx, void **vals_f16);
+/* CSR -> dense into a caller buffer of M*K FP16 (convert_csr_to_dense,
+ * src/miscalleneous.cu:66-81; a repeated column keeps the last value). */
+TCA_API int tca_csr_to_dense(int M, int K, int nnz, const int *row_ptr, const int *col_idx,
+                             const void *vals_f16, void *mat_f16);
+/* CSR row offsets -> COO row indices (caller buffer of nnz ints). */
+TCA_API int tca_csr_to_coo(int M, int nnz, const int *row_ptr, int *row_idx);
+/* COO -> CSR into caller buffers (row_ptr M+1, col/vals nnz); entries are
+ * ordered by (row, column), stably, duplicates kept. */
+TCA_API int tca_coo_to_csr(int M, int K, int nnz, const int *row_idx, const int *col_idx,
+                           const void *vals_f16, int *row_ptr, int *col_out, void *vals_out);
+
+/* ------------------------------------------------------------------ */
+/* Host-buffer forward with the reference's calling convention
+ * (our_spmm_balanced, src/our_spmm.cu:472): copies A, B (and C when it is
+ * read) to the device, builds a plan, runs the forward n_iter times, copies C
+ * back. *elapsed_ms (may be NULL) receives the mean device time of one
+ * forward, as the reference reports it (:552-574).                       */
+/* ------------------------------------------------------------------ */
+TCA_API int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals_f16,
+                  int M, int K, int nnz, const void *h_B_f16, int N,
+                  void *h_C, int c_dtype, unsigned flags, int n_iter, double *elapsed_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TCA_SPMM_H */

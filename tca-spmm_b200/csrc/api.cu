@@ -1,0 +1,155 @@
+// api.cu -- the extern "C" entry points of libtca_spmm.so declared in
+// include/tca_spmm.h: argument checking, error strings and the host-buffer
+// forward. The kernels live in spmm_*.cu and plan.cu.
+#include <cstring>
+#include <string>
+#include "tca_internal.cuh"
+#include "plan.cuh"
+
+namespace tca {
+
+static thread_local char g_err[1024] = "";
+
+int set_error(int status, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+void clear_error() { g_err[0] = '\0'; }
+
+int check_dense_args(const void *B, int ldb, int N, const void *C, int ldc, int c_dtype, int M, int K)
+{
+    if (N < 0 || M < 0 || K < 0)
+        return set_error(TCA_ERR_INVALID_ARG, "negative size (M=%d K=%d N=%d)", M, K, N);
+    if (c_dtype != TCA_DTYPE_F16 && c_dtype != TCA_DTYPE_F32)
+        return set_error(TCA_ERR_INVALID_ARG, "c_dtype %d is not F16 or F32", c_dtype);
+    if (N > 0 && ldb < N)
+        return set_error(TCA_ERR_INVALID_ARG, "ldb (%d) < N (%d)", ldb, N);
+    if (N > 0 && ldc < N)
+        return set_error(TCA_ERR_INVALID_ARG, "ldc (%d) < N (%d)", ldc, N);
+    if (N > 0 && K > 0 && M > 0 && B == nullptr)
+        return set_error(TCA_ERR_INVALID_ARG, "B is NULL");
+    if (N > 0 && M > 0 && C == nullptr)
+        return set_error(TCA_ERR_INVALID_ARG, "C is NULL");
+    return TCA_OK;
+}
+
+} // namespace tca
+
+using namespace tca;
+
+extern "C" {
+
+const char *tca_version(void) { return "tca-spmm-b200 0.1.0 (sm_100a)"; }
+
+const char *tca_last_error_string(void) { return g_err; }
+
+const char *tca_status_string(int s)
+{
+    switch (s) {
+    case TCA_OK: return "TCA_OK";
+    case TCA_ERR_INVALID_ARG: return "TCA_ERR_INVALID_ARG";
+    case TCA_ERR_CUDA: return "TCA_ERR_CUDA";
+    case TCA_ERR_ALLOC: return "TCA_ERR_ALLOC";
+    case TCA_ERR_UNSUPPORTED: return "TCA_ERR_UNSUPPORTED";
+    case TCA_ERR_TIMEOUT: return "TCA_ERR_TIMEOUT";
+    case TCA_ERR_FORMAT: return "TCA_ERR_FORMAT";
+    case TCA_ERR_IO: return "TCA_ERR_IO";
+    default: return "TCA_ERR_UNKNOWN";
+    }
+}
+
+int tca_spmm_csr(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16, int M, int K, int nnz,
+                 const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype, float alpha, float beta,
+                 unsigned flags, tca_stream_t stream)
+{
+    clear_error();
+    TCA_TRY(check_dense_args(d_B_f16, ldb, N, d_C, ldc, c_dtype, M, K));
+    if (nnz < 0)
+        return set_error(TCA_ERR_INVALID_ARG, "nnz < 0");
+    if (M == 0 || N == 0)
+        return TCA_OK;
+    if (d_row_ptr == nullptr || (nnz > 0 && (d_col_idx == nullptr || d_vals_f16 == nullptr)))
+        return set_error(TCA_ERR_INVALID_ARG, "CSR array is NULL");
+    return launch_spmm_csr_cc(d_row_ptr, d_col_idx, (const __half *)d_vals_f16, M, K, nnz,
+                              (const __half *)d_B_f16, ldb, N, d_C, ldc, c_dtype, alpha, beta, flags,
+                              (cudaStream_t)stream);
+}
+
+// Host-buffer forward: the reference's calling convention (our_spmm_balanced,
+// src/our_spmm.cu:472-588) -- device buffers are allocated and freed per call,
+// C is uploaded only when it is read (beta-free reference semantics read it for
+// the rows that stay untouched), and elapsed_ms receives the mean device time
+// of one forward over n_iter back-to-back launches.
+int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals_f16, int M, int K, int nnz,
+                  const void *h_B_f16, int N, void *h_C, int c_dtype, unsigned flags, int n_iter,
+                  double *elapsed_ms)
+{
+    clear_error();
+    TCA_TRY(check_dense_args(h_B_f16, N, N, h_C, N, c_dtype, M, K));
+    if (nnz < 0 || h_row_ptr == nullptr || (nnz > 0 && (!h_col_idx || !h_vals_f16)))
+        return set_error(TCA_ERR_INVALID_ARG, "invalid CSR arguments");
+    if (n_iter < 1)
+        n_iter = 1;
+    if (M == 0 || N == 0) {
+        if (elapsed_ms) *elapsed_ms = 0.0;
+        return TCA_OK;
+    }
+    const size_t c_elem = (c_dtype == TCA_DTYPE_F16) ? 2 : 4;
+    int *d_rp = nullptr, *d_ci = nullptr;
+    __half *d_v = nullptr, *d_B = nullptr;
+    void *d_C = nullptr;
+    tca_plan_t plan = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int st = TCA_OK;
+    auto fail_cuda = [&](cudaError_t e, const char *what) {
+        st = set_error(TCA_ERR_CUDA, "%s failed: %s", what, cudaGetErrorString(e));
+    };
+    do {
+        cudaError_t e;
+        if ((e = cudaMalloc(&d_rp, sizeof(int) * (size_t)(M + 1))) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
+        if ((e = cudaMalloc(&d_ci, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1))) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
+        if ((e = cudaMalloc(&d_v, 2 * (size_t)(nnz > 0 ? nnz : 1))) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
+        if ((e = cudaMalloc(&d_B, 2 * (size_t)(K > 0 ? K : 1) * N)) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
+        if ((e = cudaMalloc(&d_C, c_elem * (size_t)M * N)) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
+        if ((e = cudaMemcpy(d_rp, h_row_ptr, sizeof(int) * (size_t)(M + 1), cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+        if (nnz > 0) {
+            if ((e = cudaMemcpy(d_ci, h_col_idx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+            if ((e = cudaMemcpy(d_v, h_vals_f16, 2 * (size_t)nnz, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+        }
+        if (K > 0 && (e = cudaMemcpy(d_B, h_B_f16, 2 * (size_t)K * N, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+        if (flags & TCA_FLAG_KEEP_EMPTY_ROWS) {
+            if ((e = cudaMemcpy(d_C, h_C, c_elem * (size_t)M * N, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+        }
+        tca_plan_opts_t opts;
+        tca_plan_opts_default(&opts);
+        st = tca_plan_create(d_rp, d_ci, d_v, M, K, nnz, &opts, nullptr, &plan);
+        if (st != TCA_OK) break;
+        if ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess) { fail_cuda(e, "cudaEventCreate"); break; }
+        if ((e = cudaEventRecord(e0, nullptr)) != cudaSuccess) { fail_cuda(e, "cudaEventRecord"); break; }
+        for (int it = 0; it < n_iter && st == TCA_OK; it++)
+            st = tca_spmm(plan, d_B, N, N, d_C, N, c_dtype, 1.0f, 0.0f, flags, nullptr);
+        if (st != TCA_OK) break;
+        if ((e = cudaEventRecord(e1, nullptr)) != cudaSuccess) { fail_cuda(e, "cudaEventRecord"); break; }
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) { fail_cuda(e, "cudaEventSynchronize"); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (elapsed_ms) *elapsed_ms = (double)ms / n_iter;
+        if ((e = cudaMemcpy(h_C, d_C, c_elem * (size_t)M * N, cudaMemcpyDeviceToHost)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+    } while (0);
+    if (plan) tca_plan_destroy(plan);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d_rp);
+    cudaFree(d_ci);
+    cudaFree(d_v);
+    cudaFree(d_B);
+    cudaFree(d_C);
+    return st;
+}
+
+} // extern "C"

@@ -1,0 +1,728 @@
+// plan.cu -- GPU builder of the row-window, column-condensed tile format,
+// plan management and the planned forward (tca_spmm).
+//
+// This replaces the reference's per-call host schedule, workload_manager
+// (src/our_spmm.cu:347-471), which bins each row's nnz into a warp count and
+// first-fit packs rows into 8-warp thread blocks on the CPU at every call.
+// Here the schedule is built once per sparsity pattern, on the GPU, and every
+// step is deterministic (stable radix sort, prefix scans, no order-dependent
+// atomics), so a host restatement reproduces it bit for bit:
+//   1. check the CSR, count each row, flag rows with strictly increasing columns;
+//   2. order rows by nnz (descending, ties by row index) and re-order the CSR;
+//   3. per 128-row window: distinct columns (a shared-memory bitmap), nnz,
+//      eligibility (all rows strictly increasing);
+//   4. on the host: a window goes to tensor cores when it is eligible and
+//      nnz_w >= tc_min_density * 128 * 64 * ceil(distinct_w / 64);
+//   5. per tensor-core window: condensed column list and per-chunk nonzero
+//      entries packed as (local_row << 22 | local_col << 16 | fp16 bits).
+#include <cub/cub.cuh>
+#include <vector>
+#include <algorithm>
+#include "tca_internal.cuh"
+#include "plan.cuh"
+
+namespace tca {
+namespace {
+
+constexpr int kErrRowPtr = 1, kErrColRange = 2;
+
+// 1. Row checks: one warp per row.
+__global__ void k_row_check(const int *__restrict__ row_ptr, const int *__restrict__ col, int M, int K, int nnz,
+                            int *__restrict__ row_nnz, int *__restrict__ row_sorted, int *__restrict__ err)
+{
+    const int lane = threadIdx.x & 31;
+    const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= M)
+        return;
+    const int s = row_ptr[r], e = row_ptr[r + 1];
+    if (s < 0 || e < s || e > nnz || (r == 0 && s != 0) || (r == M - 1 && e != nnz)) {
+        if (lane == 0) {
+            atomicOr(err, kErrRowPtr);
+            row_nnz[r] = 0;
+            row_sorted[r] = 0;
+        }
+        return;
+    }
+    bool ok = true, inc = true;
+    for (int j = s + lane; j < e; j += 32) {
+        const int c = col[j];
+        ok &= (c >= 0 && c < K);
+        if (j > s)
+            inc &= (col[j - 1] < c);
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    inc = __all_sync(0xffffffffu, inc);
+    if (lane == 0) {
+        if (!ok)
+            atomicOr(err, kErrColRange);
+        row_nnz[r] = e - s;
+        row_sorted[r] = inc ? 1 : 0;
+    }
+}
+
+__global__ void k_iota(int *a, int n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        a[i] = (int)i;
+}
+
+__global__ void k_gather_int(const int *__restrict__ src, const int *__restrict__ idx, int *__restrict__ dst, int n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        dst[i] = src[idx[i]];
+}
+
+// 2b. Re-order the CSR: one warp per sorted row.
+__global__ void k_permute(const int *__restrict__ perm, const int *__restrict__ row_ptr,
+                          const int *__restrict__ col, const __half *__restrict__ val,
+                          const int *__restrict__ p_row_ptr, int M, int *__restrict__ p_col,
+                          __half *__restrict__ p_val, int *__restrict__ src)
+{
+    const int lane = threadIdx.x & 31;
+    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= M)
+        return;
+    const int r = perm[i];
+    const int s = row_ptr[r], e = row_ptr[r + 1], d = p_row_ptr[i];
+    for (int j = lane; j < e - s; j += 32) {
+        p_col[d + j] = col[s + j];
+        p_val[d + j] = val[s + j];
+        src[d + j] = s + j;
+    }
+}
+
+// 3. Window statistics: one block per window, K-bit bitmap in shared memory.
+__global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
+                               const int *__restrict__ p_sorted, int M, int K, int *__restrict__ win_nu,
+                               int *__restrict__ win_nnz, int *__restrict__ win_elig)
+{
+    extern __shared__ uint32_t bm[];
+    __shared__ int s_cnt, s_elig;
+    const int w = blockIdx.x;
+    const int nwords = (K + 31) >> 5;
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
+    if (threadIdx.x == 0) { s_cnt = 0; s_elig = 1; }
+    __syncthreads();
+    const int r0 = w * kWindowRows, r1 = min(M, r0 + kWindowRows);
+    const int lo = p_row_ptr[r0], hi = p_row_ptr[r1];
+    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        const int c = p_col[j];
+        atomicOr(&bm[c >> 5], 1u << (c & 31));
+    }
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+        if (!p_sorted[i]) atomicAnd(&s_elig, 0);
+    __syncthreads();
+    int cnt = 0;
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x) cnt += __popc(bm[i]);
+    atomicAdd(&s_cnt, cnt); // integer sum: order-independent
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        win_nu[w] = s_cnt;
+        win_nnz[w] = hi - lo;
+        win_elig[w] = s_elig;
+    }
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim.x == 128).
+__device__ int block_exclusive_scan128(int v, int *total, int *scratch /* >= 5 ints */)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) scratch[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int k = 0; k < 4; k++) { const int t = scratch[k]; scratch[k] = run; run += t; }
+        scratch[4] = run;
+    }
+    __syncthreads();
+    const int res = x - v + scratch[warp];
+    *total = scratch[4];
+    __syncthreads();
+    return res;
+}
+
+// 5. Tile fill: one block of 128 threads per tensor-core window.
+__global__ void __launch_bounds__(128)
+k_tile_fill(const int *__restrict__ tc_windows, const int *__restrict__ tile_first,
+            const long long *__restrict__ entry_base, const int *__restrict__ p_row_ptr,
+            const int *__restrict__ p_col, const __half *__restrict__ p_val, int M, int K,
+            int *__restrict__ win_cols, int *__restrict__ tile_ptr, uint32_t *__restrict__ entries,
+            int *__restrict__ tile_src)
+{
+    extern __shared__ uint32_t sm[];
+    __shared__ int scratch[8];
+    const int nwords = (K + 31) >> 5;
+    uint32_t *bm = sm;
+    int *pre = reinterpret_cast<int *>(sm + nwords);
+    const int t = blockIdx.x;
+    const int w = tc_windows[t];
+    const int c0 = tile_first[t], nch = tile_first[t + 1] - c0;
+    const int r0 = w * kWindowRows, r1 = min(M, r0 + kWindowRows);
+    const int lo = p_row_ptr[r0], hi = p_row_ptr[r1];
+
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
+    __syncthreads();
+    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
+        const int c = p_col[j];
+        atomicOr(&bm[c >> 5], 1u << (c & 31));
+    }
+    __syncthreads();
+    // exclusive prefix of popcounts over words: each thread owns a contiguous segment
+    const int seg = (nwords + 127) / 128;
+    const int wb = min(nwords, (int)threadIdx.x * seg), we = min(nwords, wb + seg);
+    int local = 0;
+    for (int i = wb; i < we; i++) local += __popc(bm[i]);
+    int nu;
+    int run = block_exclusive_scan128(local, &nu, scratch);
+    for (int i = wb; i < we; i++) { pre[i] = run; run += __popc(bm[i]); }
+    __syncthreads();
+    // condensed column list (ascending), padded with -1 to a multiple of 64
+    int *wc = win_cols + (size_t)c0 * kChunkCols;
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x) {
+        uint32_t b = bm[i];
+        int rk = pre[i];
+        while (b) {
+            const int bit = __ffs(b) - 1;
+            wc[rk++] = i * 32 + bit;
+            b &= b - 1;
+        }
+    }
+    for (int k = nu + threadIdx.x; k < nch * kChunkCols; k += blockDim.x) wc[k] = -1;
+
+    // per chunk: each thread owns one local row and walks its sorted columns
+    const int lr = threadIdx.x;
+    const int i = r0 + lr;
+    int cur = 0, end = 0;
+    if (i < r1) { cur = p_row_ptr[i]; end = p_row_ptr[i + 1]; }
+    long long base = entry_base[t];
+    for (int c = 0; c < nch; c++) {
+        const int lim = (c + 1) * kChunkCols;
+        int cnt = 0;
+        while (cur + cnt < end) {
+            const int col = p_col[cur + cnt];
+            const int rk = pre[col >> 5] + __popc(bm[col >> 5] & ((1u << (col & 31)) - 1u));
+            if (rk >= lim) break;
+            cnt++;
+        }
+        int total;
+        const int off = block_exclusive_scan128(cnt, &total, scratch);
+        for (int e = 0; e < cnt; e++) {
+            const int j = cur + e;
+            const int col = p_col[j];
+            const int rk = pre[col >> 5] + __popc(bm[col >> 5] & ((1u << (col & 31)) - 1u)) - c * kChunkCols;
+            const uint32_t bits = __half_as_ushort(p_val[j]);
+            entries[base + off + e] = ((uint32_t)lr << 22) | ((uint32_t)rk << 16) | bits;
+            tile_src[base + off + e] = j;
+        }
+        if (threadIdx.x == 0) tile_ptr[c0 + c] = (int)base;
+        base += total;
+        cur += cnt;
+    }
+    if (threadIdx.x == 0) tile_ptr[c0 + nch] = (int)base;
+}
+
+__global__ void k_update_p_val(const int *__restrict__ src, const __half *__restrict__ vals, __half *__restrict__ p_val, int n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        p_val[i] = vals[src[i]];
+}
+
+__global__ void k_update_entries(const int *__restrict__ tile_src, const __half *__restrict__ p_val,
+                                 uint32_t *__restrict__ entries, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        entries[i] = (entries[i] & 0xffff0000u) | (uint32_t)__half_as_ushort(p_val[tile_src[i]]);
+}
+
+// Dense tile images: one block per image chunk; zero the 128 x 64 tile, then
+// place every entry at its 128-byte-swizzled K-major position (positions are
+// distinct within a chunk, so the result does not depend on thread order).
+__global__ void __launch_bounds__(256)
+k_render_images(const int *__restrict__ img_chunk, const int *__restrict__ tile_ptr,
+                const uint32_t *__restrict__ entries, uint16_t *__restrict__ images)
+{
+    const int m = blockIdx.x;
+    const int c = img_chunk[m];
+    uint8_t *img = reinterpret_cast<uint8_t *>(images + (size_t)m * kWindowRows * kChunkCols);
+    for (int k = threadIdx.x; k < kWindowRows * kChunkCols * 2 / 16; k += blockDim.x)
+        reinterpret_cast<uint4 *>(img)[k] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    for (int e = tile_ptr[c] + threadIdx.x; e < tile_ptr[c + 1]; e += blockDim.x) {
+        const uint32_t v = entries[e];
+        *reinterpret_cast<uint16_t *>(img + swz128_offset(v >> 22, (v >> 16) & 63u)) = (uint16_t)(v & 0xffffu);
+    }
+}
+
+unsigned blocks_for(long long n, int per) { return (unsigned)((n + per - 1) / per); }
+
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
+template <typename T>
+int dev_alloc(T **ptr, size_t count, size_t *bytes)
+{
+    const size_t b = sizeof(T) * (count > 0 ? count : 1);
+    cudaError_t e = cudaMalloc((void **)ptr, b);
+    if (e != cudaSuccess)
+        return set_error(TCA_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+    if (bytes) *bytes += b;
+    return TCA_OK;
+}
+
+void free_plan(tca_plan *p)
+{
+    if (!p) return;
+    void *arrs[] = {p->perm, p->p_row_ptr, p->p_col, p->p_val, p->src, p->tc_windows, p->cc_windows,
+                    p->all_windows, p->tile_first, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src,
+                    p->img_idx, p->images, p->img_chunk, p->cc_items, p->all_items, p->d_status};
+    for (void *a : arrs)
+        if (a) cudaFree(a);
+    delete p;
+}
+
+// CUDA-core work items over the rows of `windows` (host, deterministic):
+// maximal runs of consecutive listed rows are cut greedily into items of at
+// most kItemRows rows whose nonzeros stay within kItemNnz (a row above that
+// is an item of its own).
+void build_items(const std::vector<int> &windows, const std::vector<int> &row_ptr, int M, std::vector<int2> &items)
+{
+    items.clear();
+    size_t w = 0;
+    while (w < windows.size()) {
+        const int a = windows[w] * kWindowRows;
+        size_t v = w + 1;
+        while (v < windows.size() && windows[v] == windows[v - 1] + 1) v++;
+        const int b = std::min(M, windows[v - 1] * kWindowRows + kWindowRows);
+        int i = a;
+        while (i < b) {
+            const int r0 = i;
+            int nz = row_ptr[i + 1] - row_ptr[i];
+            i++;
+            while (i < b && i - r0 < kItemRows && nz + (row_ptr[i + 1] - row_ptr[i]) <= kItemNnz) {
+                nz += row_ptr[i + 1] - row_ptr[i];
+                i++;
+            }
+            items.push_back(make_int2(r0, i));
+        }
+        w = v;
+    }
+}
+
+int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *val, cudaStream_t s)
+{
+    const int M = p->M, K = p->K, nnz = p->nnz;
+    size_t *bytes = &p->bytes;
+    DevBuf t_row_nnz, t_row_sorted, t_err, t_iota, t_keys_out, t_p_sorted, t_scan_in, t_cub;
+    int *row_nnz, *row_sorted, *err, *iota, *keys_out, *p_sorted, *scan_in;
+    TCA_TRY(dev_alloc(&row_nnz, M, nullptr)); t_row_nnz.p = row_nnz;
+    TCA_TRY(dev_alloc(&row_sorted, M, nullptr)); t_row_sorted.p = row_sorted;
+    TCA_TRY(dev_alloc(&err, 1, nullptr)); t_err.p = err;
+    TCA_TRY(dev_alloc(&iota, M, nullptr)); t_iota.p = iota;
+    TCA_TRY(dev_alloc(&keys_out, M, nullptr)); t_keys_out.p = keys_out;
+    TCA_TRY(dev_alloc(&p_sorted, M, nullptr)); t_p_sorted.p = p_sorted;
+    TCA_TRY(dev_alloc(&scan_in, M + 1, nullptr)); t_scan_in.p = scan_in;
+
+    TCA_TRY(dev_alloc(&p->perm, M, bytes));
+    TCA_TRY(dev_alloc(&p->p_row_ptr, M + 1, bytes));
+    TCA_TRY(dev_alloc(&p->p_col, nnz, bytes));
+    TCA_TRY(dev_alloc(&p->p_val, nnz, bytes));
+    TCA_TRY(dev_alloc(&p->src, nnz, bytes));
+    TCA_TRY(dev_alloc(&p->d_status, 1, bytes));
+    TCA_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, sizeof(int), s));
+    TCA_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
+
+    // 1. checks
+    k_row_check<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(row_ptr, col, M, K, nnz, row_nnz, row_sorted, err);
+    TCA_CUDA_TRY(cudaGetLastError());
+    int h_err = 0;
+    TCA_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h_err & kErrRowPtr)
+        return set_error(TCA_ERR_FORMAT, "row_ptr is not a valid CSR offset array (must start at 0, be non-decreasing and end at nnz=%d)", nnz);
+    if (h_err & kErrColRange)
+        return set_error(TCA_ERR_FORMAT, "a column index lies outside [0, K=%d)", K);
+
+    // 2. row order
+    k_iota<<<blocks_for(M, 256), 256, 0, s>>>(iota, M);
+    if (p->opts.sort_rows) {
+        size_t tmp = 0;
+        TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, row_nnz, keys_out, iota, p->perm, M, 0, 32, s));
+        void *tbuf;
+        TCA_TRY(dev_alloc((char **)&tbuf, tmp, nullptr)); t_cub.p = tbuf;
+        TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, row_nnz, keys_out, iota, p->perm, M, 0, 32, s));
+    } else {
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->perm, iota, sizeof(int) * M, cudaMemcpyDeviceToDevice, s));
+    }
+    TCA_CUDA_TRY(cudaMemsetAsync(scan_in + M, 0, sizeof(int), s));
+    k_gather_int<<<blocks_for(M, 256), 256, 0, s>>>(row_nnz, p->perm, scan_in, M);
+    k_gather_int<<<blocks_for(M, 256), 256, 0, s>>>(row_sorted, p->perm, p_sorted, M);
+    {
+        size_t tmp = 0;
+        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, scan_in, p->p_row_ptr, M + 1, s));
+        DevBuf tb;
+        char *tbuf;
+        TCA_TRY(dev_alloc(&tbuf, tmp, nullptr)); tb.p = tbuf;
+        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tbuf, tmp, scan_in, p->p_row_ptr, M + 1, s));
+        TCA_CUDA_TRY(cudaStreamSynchronize(s)); // tb is freed at scope exit
+    }
+    k_permute<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(p->perm, row_ptr, col, val, p->p_row_ptr, M,
+                                                                 p->p_col, p->p_val, p->src);
+    TCA_CUDA_TRY(cudaGetLastError());
+
+    // 3. windows
+    const int W = (M + kWindowRows - 1) / kWindowRows;
+    p->n_windows = W;
+    std::vector<int> h_all(W);
+    for (int w = 0; w < W; w++) h_all[w] = w;
+    TCA_TRY(dev_alloc(&p->all_windows, W, bytes));
+    TCA_CUDA_TRY(cudaMemcpyAsync(p->all_windows, h_all.data(), sizeof(int) * W, cudaMemcpyHostToDevice, s));
+
+    std::vector<int> h_nu(W, 0), h_nnz(W, 0), h_elig(W, 0);
+    const bool tc_possible = (p->opts.path != 1) && K <= kMaxTcK && K > 0 && W > 0;
+    if (tc_possible) {
+        DevBuf t_nu, t_wn, t_el;
+        int *d_nu, *d_wn, *d_el;
+        TCA_TRY(dev_alloc(&d_nu, W, nullptr)); t_nu.p = d_nu;
+        TCA_TRY(dev_alloc(&d_wn, W, nullptr)); t_wn.p = d_wn;
+        TCA_TRY(dev_alloc(&d_el, W, nullptr)); t_el.p = d_el;
+        const size_t smem = sizeof(uint32_t) * ((K + 31) / 32);
+        TCA_CUDA_TRY(cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_window_stats<<<W, 256, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, d_nu, d_wn, d_el);
+        TCA_CUDA_TRY(cudaGetLastError());
+        TCA_CUDA_TRY(cudaMemcpyAsync(h_nu.data(), d_nu, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
+        TCA_CUDA_TRY(cudaMemcpyAsync(h_nnz.data(), d_wn, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
+        TCA_CUDA_TRY(cudaMemcpyAsync(h_elig.data(), d_el, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
+        TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+
+    // 4. path decision (host, deterministic)
+    std::vector<int> tc_list, cc_list, h_first(1, 0);
+    std::vector<long long> h_ebase;
+    long long ebase = 0;
+    for (int w = 0; w < W; w++) {
+        const int nch = (h_nu[w] + kChunkCols - 1) / kChunkCols;
+        bool tc = false;
+        if (tc_possible && h_elig[w] && h_nnz[w] > 0) {
+            if (p->opts.path == 2)
+                tc = true;
+            else
+                tc = (double)h_nnz[w] >= (double)p->opts.tc_min_density * (double)(kWindowRows * kChunkCols) * (double)nch;
+        }
+        if (tc) {
+            tc_list.push_back(w);
+            h_first.push_back(h_first.back() + nch);
+            h_ebase.push_back(ebase);
+            ebase += h_nnz[w];
+        } else {
+            cc_list.push_back(w);
+        }
+    }
+    p->n_tc = (int)tc_list.size();
+    p->n_cc = (int)cc_list.size();
+    p->n_tc_chunks = h_first.back();
+    p->tc_nnz = ebase;
+    TCA_TRY(dev_alloc(&p->tc_windows, p->n_tc, bytes));
+    TCA_TRY(dev_alloc(&p->cc_windows, p->n_cc, bytes));
+    TCA_TRY(dev_alloc(&p->tile_first, p->n_tc + 1, bytes));
+    if (p->n_tc)
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->tc_windows, tc_list.data(), sizeof(int) * p->n_tc, cudaMemcpyHostToDevice, s));
+    if (p->n_cc)
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->cc_windows, cc_list.data(), sizeof(int) * p->n_cc, cudaMemcpyHostToDevice, s));
+    TCA_CUDA_TRY(cudaMemcpyAsync(p->tile_first, h_first.data(), sizeof(int) * (p->n_tc + 1), cudaMemcpyHostToDevice, s));
+
+    // 5. tiles
+    TCA_TRY(dev_alloc(&p->win_cols, (size_t)p->n_tc_chunks * kChunkCols, bytes));
+    TCA_TRY(dev_alloc(&p->tile_ptr, (size_t)p->n_tc_chunks + 1, bytes));
+    TCA_TRY(dev_alloc(&p->tile_entries, (size_t)p->tc_nnz + kEntryPad, bytes));
+    TCA_CUDA_TRY(cudaMemsetAsync(p->tile_entries + p->tc_nnz, 0, sizeof(uint32_t) * kEntryPad, s));
+    TCA_TRY(dev_alloc(&p->tile_src, (size_t)p->tc_nnz, bytes));
+    if (p->n_tc > 0) {
+        DevBuf t_eb;
+        long long *d_eb;
+        TCA_TRY(dev_alloc(&d_eb, p->n_tc, nullptr)); t_eb.p = d_eb;
+        TCA_CUDA_TRY(cudaMemcpyAsync(d_eb, h_ebase.data(), sizeof(long long) * p->n_tc, cudaMemcpyHostToDevice, s));
+        const size_t smem = 2 * sizeof(uint32_t) * ((K + 31) / 32);
+        TCA_CUDA_TRY(cudaFuncSetAttribute(k_tile_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_tile_fill<<<p->n_tc, 128, smem, s>>>(p->tc_windows, p->tile_first, d_eb, p->p_row_ptr, p->p_col, p->p_val,
+                                               M, K, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src);
+        TCA_CUDA_TRY(cudaGetLastError());
+        TCA_CUDA_TRY(cudaStreamSynchronize(s)); // d_eb is freed at scope exit
+    } else {
+        TCA_CUDA_TRY(cudaMemsetAsync(p->tile_ptr, 0, sizeof(int), s));
+    }
+
+    // 6. dense tile images for chunks holding at least half a tile of nonzeros
+    std::vector<int> h_ptr((size_t)p->n_tc_chunks + 1, 0), h_img((size_t)p->n_tc_chunks, -1), h_img_chunk;
+    if (p->n_tc_chunks > 0)
+        TCA_CUDA_TRY(cudaMemcpyAsync(h_ptr.data(), p->tile_ptr, sizeof(int) * h_ptr.size(), cudaMemcpyDeviceToHost, s));
+    TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int c = 0; c < p->n_tc_chunks; c++)
+        if (h_ptr[c + 1] - h_ptr[c] >= kImageMinNnz) {
+            h_img[c] = (int)h_img_chunk.size();
+            h_img_chunk.push_back(c);
+        }
+    p->n_images = (int)h_img_chunk.size();
+    TCA_TRY(dev_alloc(&p->img_idx, (size_t)p->n_tc_chunks, bytes));
+    TCA_TRY(dev_alloc(&p->img_chunk, (size_t)p->n_images, bytes));
+    TCA_TRY(dev_alloc(&p->images, (size_t)p->n_images * kWindowRows * kChunkCols, bytes));
+    if (p->n_tc_chunks > 0)
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->img_idx, h_img.data(), sizeof(int) * h_img.size(), cudaMemcpyHostToDevice, s));
+    if (p->n_images > 0) {
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->img_chunk, h_img_chunk.data(), sizeof(int) * h_img_chunk.size(),
+                                     cudaMemcpyHostToDevice, s));
+        k_render_images<<<p->n_images, 256, 0, s>>>(p->img_chunk, p->tile_ptr, p->tile_entries, p->images);
+        TCA_CUDA_TRY(cudaGetLastError());
+    }
+
+    // 7. CUDA-core work items
+    std::vector<int> h_rp((size_t)M + 1);
+    TCA_CUDA_TRY(cudaMemcpyAsync(h_rp.data(), p->p_row_ptr, sizeof(int) * h_rp.size(), cudaMemcpyDeviceToHost, s));
+    TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<int2> items;
+    build_items(cc_list, h_rp, M, items);
+    p->n_cc_items = (int)items.size();
+    TCA_TRY(dev_alloc(&p->cc_items, items.size(), bytes));
+    if (!items.empty())
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->cc_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
+    TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    build_items(h_all, h_rp, M, items);
+    p->n_all_items = (int)items.size();
+    TCA_TRY(dev_alloc(&p->all_items, items.size(), bytes));
+    if (!items.empty())
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->all_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
+    TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    return TCA_OK;
+}
+
+} // namespace
+} // namespace tca
+
+using namespace tca;
+
+extern "C" {
+
+void tca_plan_opts_default(tca_plan_opts_t *o)
+{
+    if (!o) return;
+    *o = tca_plan_opts_t{};
+    o->sort_rows = 1;
+    o->tc_min_density = 0.02f;
+    o->path = 0;
+}
+
+int tca_plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16, int M, int K, int nnz,
+                    const tca_plan_opts_t *opts, tca_stream_t stream, tca_plan_t *plan)
+{
+    clear_error();
+    if (!plan)
+        return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    *plan = nullptr;
+    if (M < 0 || K < 0 || nnz < 0)
+        return set_error(TCA_ERR_INVALID_ARG, "negative size (M=%d K=%d nnz=%d)", M, K, nnz);
+    if ((M > 0 && !d_row_ptr) || (nnz > 0 && (!d_col_idx || !d_vals_f16)))
+        return set_error(TCA_ERR_INVALID_ARG, "CSR array is NULL");
+    tca_plan_opts_t o;
+    tca_plan_opts_default(&o);
+    if (opts) o = *opts;
+    if (o.path < 0 || o.path > 2 || !(o.tc_min_density >= 0.f))
+        return set_error(TCA_ERR_INVALID_ARG, "invalid plan options");
+    tca_plan *p = new (std::nothrow) tca_plan();
+    if (!p)
+        return set_error(TCA_ERR_ALLOC, "host allocation failed");
+    p->M = M; p->K = K; p->nnz = nnz; p->opts = o;
+    int st = TCA_OK;
+    if (M > 0)
+        st = build_plan(p, d_row_ptr, d_col_idx, (const __half *)d_vals_f16, (cudaStream_t)stream);
+    if (st != TCA_OK) {
+        free_plan(p);
+        return st;
+    }
+    *plan = p;
+    return TCA_OK;
+}
+
+int tca_plan_update_values(tca_plan_t p, const void *d_vals_f16, tca_stream_t stream)
+{
+    clear_error();
+    if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    if (p->nnz == 0) return TCA_OK;
+    if (!d_vals_f16) return set_error(TCA_ERR_INVALID_ARG, "values are NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    k_update_p_val<<<blocks_for(p->nnz, 256), 256, 0, s>>>(p->src, (const __half *)d_vals_f16, p->p_val, p->nnz);
+    if (p->tc_nnz > 0)
+        k_update_entries<<<blocks_for(p->tc_nnz, 256), 256, 0, s>>>(p->tile_src, p->p_val, p->tile_entries, p->tc_nnz);
+    if (p->n_images > 0)
+        k_render_images<<<p->n_images, 256, 0, s>>>(p->img_chunk, p->tile_ptr, p->tile_entries, p->images);
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
+int tca_plan_info(tca_plan_t p, tca_plan_info_t *info)
+{
+    clear_error();
+    if (!p || !info) return set_error(TCA_ERR_INVALID_ARG, "NULL argument");
+    *info = tca_plan_info_t{};
+    info->M = p->M; info->K = p->K; info->nnz = p->nnz;
+    info->n_windows = p->n_windows;
+    info->n_tc_windows = p->n_tc;
+    info->n_cc_windows = p->n_cc;
+    info->n_tc_chunks = p->n_tc_chunks;
+    info->tc_nnz = p->tc_nnz;
+    info->format_bytes = (long long)p->bytes;
+    info->n_images = p->n_images;
+    return TCA_OK;
+}
+
+int tca_plan_export(tca_plan_t p, int which, void *h_dst, size_t capacity, size_t *out_bytes)
+{
+    clear_error();
+    if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    const void *src = nullptr;
+    size_t n = 0;
+    switch (which) {
+    case TCA_ARR_ROW_PERM: src = p->perm; n = sizeof(int) * p->M; break;
+    case TCA_ARR_P_ROW_PTR: src = p->p_row_ptr; n = p->M > 0 ? sizeof(int) * (p->M + 1) : 0; break;
+    case TCA_ARR_P_COL: src = p->p_col; n = sizeof(int) * p->nnz; break;
+    case TCA_ARR_P_VAL: src = p->p_val; n = 2 * (size_t)p->nnz; break;
+    case TCA_ARR_SRC: src = p->src; n = sizeof(int) * p->nnz; break;
+    case TCA_ARR_TC_WINDOWS: src = p->tc_windows; n = sizeof(int) * p->n_tc; break;
+    case TCA_ARR_CC_WINDOWS: src = p->cc_windows; n = sizeof(int) * p->n_cc; break;
+    case TCA_ARR_TILE_FIRST: src = p->tile_first; n = p->M > 0 ? sizeof(int) * (p->n_tc + 1) : 0; break;
+    case TCA_ARR_WIN_COLS: src = p->win_cols; n = sizeof(int) * (size_t)p->n_tc_chunks * kChunkCols; break;
+    case TCA_ARR_TILE_PTR: src = p->tile_ptr; n = p->M > 0 ? sizeof(int) * ((size_t)p->n_tc_chunks + 1) : 0; break;
+    case TCA_ARR_TILE_ENTRIES: src = p->tile_entries; n = sizeof(uint32_t) * (size_t)p->tc_nnz; break;
+    case TCA_ARR_TILE_SRC: src = p->tile_src; n = sizeof(int) * (size_t)p->tc_nnz; break;
+    case TCA_ARR_TILE_IMAGE_IDX: src = p->img_idx; n = sizeof(int) * (size_t)p->n_tc_chunks; break;
+    case TCA_ARR_TILE_IMAGES: src = p->images; n = sizeof(uint16_t) * (size_t)p->n_images * kWindowRows * kChunkCols; break;
+    case TCA_ARR_CC_ITEMS: src = p->cc_items; n = sizeof(int2) * (size_t)p->n_cc_items; break;
+    case TCA_ARR_ALL_ITEMS: src = p->all_items; n = sizeof(int2) * (size_t)p->n_all_items; break;
+    default: return set_error(TCA_ERR_INVALID_ARG, "unknown plan array %d", which);
+    }
+    if (out_bytes) *out_bytes = n;
+    if (!h_dst || n == 0) return TCA_OK;
+    if (capacity < n) return set_error(TCA_ERR_INVALID_ARG, "destination holds %zu bytes, %zu needed", capacity, n);
+    TCA_CUDA_TRY(cudaMemcpy(h_dst, src, n, cudaMemcpyDeviceToHost));
+    return TCA_OK;
+}
+
+int tca_plan_status(tca_plan_t p)
+{
+    clear_error();
+    if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    if (!p->d_status) return TCA_OK;
+    int h = 0;
+    TCA_CUDA_TRY(cudaMemcpy(&h, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h & kStatusTimeout)
+        return set_error(TCA_ERR_TIMEOUT, "a bounded device-side wait gave up (status word 0x%x)", h);
+    return TCA_OK;
+}
+
+int tca_plan_destroy(tca_plan_t p)
+{
+    clear_error();
+    free_plan(p);
+    return TCA_OK;
+}
+
+static int make_job(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype,
+                    bool batched, SpmmJob *job)
+{
+    if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    TCA_TRY(check_dense_args(d_B_f16, ldb, N, d_C, ldc, c_dtype, p->M, p->K));
+    job->p = p;
+    job->B = (const __half *)d_B_f16;
+    job->C = d_C;
+    job->ldb = ldb;
+    job->N = N;
+    job->ldc = ldc;
+    job->tc = p->n_tc > 0 && dense_operands_vec_ok(d_B_f16, ldb, N, d_C, ldc, c_dtype);
+    job->n_tile = pick_tc_tile(p->n_tc, N, batched);
+    return TCA_OK;
+}
+
+static int spmm_impl(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype,
+                     float alpha, float beta, unsigned flags, cudaStream_t s, void *const *ev)
+{
+    clear_error();
+    SpmmJob job;
+    TCA_TRY(make_job(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, false, &job));
+    if (p->M == 0 || N == 0) return TCA_OK;
+    auto rec = [&](int i) -> int {
+        if (ev && ev[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)ev[i], s));
+        return TCA_OK;
+    };
+    TCA_TRY(rec(0));
+    TCA_TRY(launch_tc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
+    TCA_TRY(rec(1));
+    TCA_TRY(rec(2));
+    TCA_TRY(launch_cc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
+    TCA_TRY(rec(3));
+    return TCA_OK;
+}
+
+int tca_spmm(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype, float alpha,
+             float beta, unsigned flags, tca_stream_t stream)
+{
+    return spmm_impl(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, alpha, beta, flags, (cudaStream_t)stream, nullptr);
+}
+
+int tca_spmm_events(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype,
+                    float alpha, float beta, unsigned flags, tca_stream_t stream, void *const *events)
+{
+    return spmm_impl(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, alpha, beta, flags, (cudaStream_t)stream, events);
+}
+
+int tca_spmm_batched(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
+                     unsigned flags, tca_stream_t stream, void *const *events)
+{
+    clear_error();
+    if (n_items < 0 || (n_items > 0 && !items))
+        return set_error(TCA_ERR_INVALID_ARG, "invalid batch");
+    std::vector<SpmmJob> jobs;
+    jobs.reserve((size_t)n_items);
+    for (int i = 0; i < n_items; i++) {
+        SpmmJob j;
+        const tca_batch_item_t &it = items[i];
+        TCA_TRY(make_job(it.plan, it.d_B_f16, it.ldb, it.N, it.d_C, it.ldc, c_dtype, true, &j));
+        if (it.n_tile == 64 || it.n_tile == 128 || it.n_tile == 256)
+            j.n_tile = it.n_tile;
+        if (it.plan->M > 0 && it.N > 0)
+            jobs.push_back(j);
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    auto rec = [&](int i) -> int {
+        if (events && events[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[i], s));
+        return TCA_OK;
+    };
+    TCA_TRY(rec(0));
+    TCA_TRY(launch_tc_jobs(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s));
+    TCA_TRY(rec(1));
+    TCA_TRY(rec(2));
+    TCA_TRY(launch_cc_jobs(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s));
+    TCA_TRY(rec(3));
+    return TCA_OK;
+}
+
+int tca_plan_launch_counts(tca_plan_t p, int N, int *n_tc_launches, int *n_cc_launches)
+{
+    clear_error();
+    if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    const bool empty = p->M == 0 || N == 0;
+    if (n_tc_launches) *n_tc_launches = (!empty && p->n_tc > 0) ? 1 : 0;
+    if (n_cc_launches) *n_cc_launches = (!empty && (p->n_tc == 0 ? p->n_windows : p->n_cc) > 0) ? 1 : 0;
+    return TCA_OK;
+}
+
+} // extern "C"

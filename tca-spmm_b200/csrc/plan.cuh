@@ -1,0 +1,109 @@
+// plan.cuh -- the row-window, column-condensed tile format (a tca_plan).
+//
+// Layout in HBM (all arrays device-resident, int32 unless stated):
+//   perm[M]            sorted position -> caller's row (rows ordered by nnz,
+//                      descending, ties by row index)
+//   p_row_ptr[M+1], p_col[nnz], p_val[nnz] (FP16), src[nnz]
+//                      the CSR re-ordered by perm; src maps each entry back to
+//                      the caller's nonzero index (for value updates)
+//   windows            w covers sorted positions [128 w, 128 w + 128)
+//   tc_windows[n_tc], cc_windows[n_cc]
+//                      windows on the tensor-core / CUDA-core path
+//   tile_first[n_tc+1] first condensed chunk of each tensor-core window
+//   win_cols[chunks*64] the window's distinct columns, ascending, 64 per chunk,
+//                      -1 padding in the last chunk
+//   tile_ptr[chunks+1], tile_entries[tc_nnz + 4] (uint32), tile_src[tc_nnz]
+//                      per chunk, its nonzeros as (local_row << 22 |
+//                      local_col << 16 | fp16 bits), ordered by (row, column);
+//                      tile_src indexes p_val; 4 zero entries of padding let
+//                      16-byte copies round the end of the last chunk up
+//   img_idx[chunks], images[n_images * 8192] (FP16)
+//                      chunks with >= 4096 nonzeros (half the tile: fewer
+//                      bytes as a dense tile than as entries) are also kept
+//                      as a dense 128 x 64 tile, already in the 128-byte
+//                      swizzled K-major layout the tensor cores read from
+//                      shared memory; img_idx is -1 for the other chunks
+#pragma once
+#include "tca_internal.cuh"
+
+struct tca_plan {
+    int M = 0, K = 0, nnz = 0;
+    int n_windows = 0, n_tc = 0, n_cc = 0, n_tc_chunks = 0;
+    long long tc_nnz = 0;
+    tca_plan_opts_t opts{};
+    int *perm = nullptr;
+    int *p_row_ptr = nullptr;
+    int *p_col = nullptr;
+    __half *p_val = nullptr;
+    int *src = nullptr;
+    int *tc_windows = nullptr;
+    int *cc_windows = nullptr;
+    int *all_windows = nullptr;
+    int *tile_first = nullptr;
+    int *win_cols = nullptr;
+    int *tile_ptr = nullptr;
+    uint32_t *tile_entries = nullptr;
+    int *tile_src = nullptr;
+    int *img_idx = nullptr;
+    int *img_chunk = nullptr; // image -> chunk
+    uint16_t *images = nullptr;
+    int n_images = 0;
+    // CUDA-core work items: runs of consecutive sorted rows [x, y) with at
+    // most kItemRows rows and kItemNnz nonzeros (a longer row is an item of
+    // its own), over the CUDA-core windows (cc_items) or over all windows
+    // (all_items, used when the tensor-core kernel cannot run).
+    int2 *cc_items = nullptr;
+    int2 *all_items = nullptr;
+    int n_cc_items = 0, n_all_items = 0;
+    int *d_status = nullptr; // device error word written by bounded waits
+    size_t bytes = 0;
+};
+
+namespace tca {
+
+constexpr int kImageMinNnz = kWindowRows * kChunkCols / 2; // 4096
+constexpr int kEntryPad = 4;
+constexpr int kItemRows = 31;
+constexpr int kItemNnz = 32;
+
+// Byte offset of element (r, c) of a 128 x 64 FP16 tile in the 128-byte
+// swizzled K-major layout: 16-byte chunk index c/8 XOR-ed with r % 8.
+__host__ __device__ inline uint32_t swz128_offset(uint32_t r, uint32_t c)
+{
+    return r * 128u + ((((c >> 3) ^ (r & 7u))) << 4) + ((c & 7u) << 1);
+}
+
+// Largest K for which windows may go to the tensor-core path: the builder
+// keeps a K-bit column bitmap plus its prefix counts in shared memory.
+constexpr int kMaxTcK = 1 << 17;
+
+// Device status bits.
+constexpr int kStatusTimeout = 1;
+
+// One forward of one plan, as the batched launchers see it.
+struct SpmmJob {
+    const tca_plan *p;
+    const __half *B;
+    void *C;
+    int ldb, N, ldc;
+    bool tc;    // the plan's tensor-core windows run on tensor cores
+    int n_tile; // tensor-core N-slice width (64, 128, 256)
+};
+
+// Tensor-core (tcgen05) forward over the tensor-core windows of every job
+// (jobs with tc set), in as few launches as the N-slice widths allow.
+int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
+                   cudaStream_t s);
+
+// CUDA-core forward over the remaining windows of every job (all windows of
+// jobs without tc), in as few launches as the row widths allow.
+int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
+                   cudaStream_t s);
+
+// The N-slice width a single forward of this plan uses.
+int pick_tc_tile(int n_tc, int N, bool batched);
+
+// Whether B/C of a forward allow the vectorised and tensor-core kernels.
+bool dense_operands_vec_ok(const void *B, int ldb, int N, const void *C, int ldc, int c_dtype);
+
+} // namespace tca

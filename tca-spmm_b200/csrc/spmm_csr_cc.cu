@@ -1,0 +1,489 @@
+// spmm_csr_cc.cu -- CSR x dense SpMM on CUDA cores.
+//
+// C[r, :] = alpha * sum_j val_j * B[col_j, :] + beta * C[r, :], FP32 accumulation.
+// This restates the computation of kernel_our_spmm_balanced
+// (src/our_spmm.cu:290-346) without its host-built warp schedule and without
+// using mma.sync as a dot-product engine: a group of LPR lanes owns one row,
+// each lane owns 8 consecutive output columns (one 16-byte vector of B), and
+// the group walks the row's nonzeros, broadcasting (col, val) pairs by shuffle
+// so that every B access is a fully used, coalesced 16-byte load with 8 loads
+// in flight per lane.
+//
+// Two kernels:
+//   * plan-free (tca_spmm_csr): group g computes caller row g straight from
+//     the CSR, 8 B loads in flight per lane;
+//   * planned (tca_spmm / tca_spmm_batched): groups stream through work items
+//     of consecutive sorted rows of one or many plans (see below).
+//
+// Malformed CSR never faults: row ranges are clamped to [0, nnz] and
+// nonzeros whose column is outside [0, K) contribute nothing.
+#include "tca_internal.cuh"
+#include "plan.cuh"
+
+namespace tca {
+namespace {
+
+__device__ __forceinline__ void fma8(float *acc, float a, const uint4 &b)
+{
+    const __half2 *h = reinterpret_cast<const __half2 *>(&b);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        float2 f = __half22float2(h[i]);
+        acc[2 * i] = fmaf(a, f.x, acc[2 * i]);
+        acc[2 * i + 1] = fmaf(a, f.y, acc[2 * i + 1]);
+    }
+}
+
+__device__ __forceinline__ void load8(const __half *p, float *v)
+{
+    uint4 u = *reinterpret_cast<const uint4 *>(p);
+    const __half2 *h = reinterpret_cast<const __half2 *>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        float2 f = __half22float2(h[i]);
+        v[2 * i] = f.x;
+        v[2 * i + 1] = f.y;
+    }
+}
+__device__ __forceinline__ void load8(const float *p, float *v)
+{
+    float4 a = reinterpret_cast<const float4 *>(p)[0];
+    float4 b = reinterpret_cast<const float4 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void store8(__half *p, const float *v)
+{
+    uint4 u;
+    __half2 *h = reinterpret_cast<__half2 *>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; i++) h[i] = __floats2half2_rn(v[2 * i], v[2 * i + 1]);
+    *reinterpret_cast<uint4 *>(p) = u;
+}
+__device__ __forceinline__ void store8(float *p, const float *v)
+{
+    reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+    reinterpret_cast<float4 *>(p)[1] = make_float4(v[4], v[5], v[6], v[7]);
+}
+
+template <typename T> __device__ __forceinline__ float to_f(T x);
+template <> __device__ __forceinline__ float to_f<__half>(__half x) { return __half2float(x); }
+template <> __device__ __forceinline__ float to_f<float>(float x) { return x; }
+template <typename T> __device__ __forceinline__ T from_f(float x);
+template <> __device__ __forceinline__ __half from_f<__half>(float x) { return __float2half_rn(x); }
+template <> __device__ __forceinline__ float from_f<float>(float x) { return x; }
+
+// One row with LPR lanes, vectorised: N % 8 == 0, ldb % 8 == 0, 16-byte
+// aligned B and C rows. Every lane of the group must call it.
+template <typename OutT, int LPR>
+__device__ __forceinline__ void row_vec(int start, int end, int K, const int *__restrict__ col_idx,
+                                        const __half *__restrict__ vals, const __half *__restrict__ B, int ldb,
+                                        int N, OutT *__restrict__ Crow, float alpha, float beta, int sub,
+                                        unsigned gmask)
+{
+    constexpr int U = 8; // nonzeros in flight per lane
+    for (int nb = 0; nb < N; nb += LPR * 8) {
+        const int n0 = nb + sub * 8;
+        const bool active = n0 < N;
+        const __half *Bn = B + (active ? n0 : 0);
+        float acc[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc[i] = 0.f;
+
+        for (int base = start; base < end; base += LPR) {
+            const int j = base + sub;
+            int c = -1;
+            float a = 0.f;
+            if (j < end) {
+                c = __ldg(col_idx + j);
+                a = __half2float(vals[j]);
+                if (c < 0 || c >= K) { c = -1; a = 0.f; }
+            }
+            const int cnt = min(LPR, end - base);
+            int t = 0;
+            for (; t + U <= cnt; t += U) {
+                uint4 bv[U];
+                float av[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int cu = __shfl_sync(gmask, c, t + u, LPR);
+                    av[u] = __shfl_sync(gmask, a, t + u, LPR);
+                    bv[u] = make_uint4(0, 0, 0, 0);
+                    if (active && cu >= 0)
+                        bv[u] = __ldg(reinterpret_cast<const uint4 *>(Bn + (size_t)cu * ldb));
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) fma8(acc, av[u], bv[u]);
+            }
+            for (; t < cnt; t++) {
+                const int cu = __shfl_sync(gmask, c, t, LPR);
+                const float au = __shfl_sync(gmask, a, t, LPR);
+                if (active && cu >= 0)
+                    fma8(acc, au, __ldg(reinterpret_cast<const uint4 *>(Bn + (size_t)cu * ldb)));
+            }
+        }
+        if (active) {
+            OutT *cp = Crow + n0;
+            float out[8];
+            if (beta != 0.f) {
+                float old[8];
+                load8(cp, old);
+#pragma unroll
+                for (int i = 0; i < 8; i++) out[i] = fmaf(alpha, acc[i], beta * old[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 8; i++) out[i] = alpha * acc[i];
+            }
+            store8(cp, out);
+        }
+    }
+}
+
+// One row with a full warp, scalar: any N, leading dimension and alignment.
+template <typename OutT>
+__device__ __forceinline__ void row_scalar(int start, int end, int K, const int *__restrict__ col_idx,
+                                           const __half *__restrict__ vals, const __half *__restrict__ B,
+                                           int ldb, int N, OutT *__restrict__ Crow, float alpha, float beta,
+                                           int lane)
+{
+    for (int nb = 0; nb < N; nb += 32) {
+        const int n = nb + lane;
+        float acc = 0.f;
+        for (int base = start; base < end; base += 32) {
+            const int j = base + lane;
+            int c = -1;
+            float a = 0.f;
+            if (j < end) {
+                c = col_idx[j];
+                a = __half2float(vals[j]);
+                if (c < 0 || c >= K) { c = -1; a = 0.f; }
+            }
+            const int cnt = min(32, end - base);
+            for (int t = 0; t < cnt; t++) {
+                const int cu = __shfl_sync(0xffffffffu, c, t);
+                const float au = __shfl_sync(0xffffffffu, a, t);
+                if (n < N && cu >= 0)
+                    acc = fmaf(au, __half2float(B[(size_t)cu * ldb + n]), acc);
+            }
+        }
+        if (n < N) {
+            float o = alpha * acc;
+            if (beta != 0.f) o = fmaf(beta, to_f<OutT>(Crow[n]), o);
+            Crow[n] = from_f<OutT>(o);
+        }
+    }
+}
+
+__device__ __forceinline__ void clamp_range(int &start, int &end, int nnz)
+{
+    start = max(0, min(start, nnz));
+    end = max(start, min(end, nnz));
+}
+
+// Plan-free: group g of LPR lanes computes caller row g.
+template <typename OutT, int LPR>
+__global__ void __launch_bounds__(256)
+spmm_csr_vec_kernel(const int *__restrict__ row_ptr, const int *__restrict__ col_idx,
+                    const __half *__restrict__ vals, int M, int K, int nnz,
+                    const __half *__restrict__ B, int ldb, int N,
+                    OutT *__restrict__ C, int ldc, float alpha, float beta, unsigned flags)
+{
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & (LPR - 1);
+    const long long group = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / LPR;
+    const unsigned gmask = (LPR == 32) ? 0xffffffffu : (((1u << LPR) - 1u) << (lane & ~(LPR - 1)));
+    if (group >= M)
+        return; // the whole group leaves together
+    const int r = (int)group;
+    int start = row_ptr[r], end = row_ptr[r + 1];
+    clamp_range(start, end, nnz);
+    if (start == end && (flags & TCA_FLAG_KEEP_EMPTY_ROWS))
+        return;
+    row_vec<OutT, LPR>(start, end, K, col_idx, vals, B, ldb, N, C + (size_t)r * ldc, alpha, beta, sub, gmask);
+}
+
+template <typename OutT>
+__global__ void __launch_bounds__(256)
+spmm_csr_scalar_kernel(const int *__restrict__ row_ptr, const int *__restrict__ col_idx,
+                       const __half *__restrict__ vals, int M, int K, int nnz,
+                       const __half *__restrict__ B, int ldb, int N,
+                       OutT *__restrict__ C, int ldc, float alpha, float beta, unsigned flags)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= M)
+        return;
+    const int r = (int)warp;
+    int start = row_ptr[r], end = row_ptr[r + 1];
+    clamp_range(start, end, nnz);
+    if (start == end && (flags & TCA_FLAG_KEEP_EMPTY_ROWS))
+        return;
+    row_scalar<OutT>(start, end, K, col_idx, vals, B, ldb, N, C + (size_t)r * ldc, alpha, beta, lane);
+}
+
+// Rows of plans, batched and streamed. Every job (one forward of one plan)
+// contributes its work items: runs of consecutive sorted rows with about
+// kItemNnz nonzeros in total. A group of L lanes takes one item and streams
+// through its nonzeros -- which are contiguous in the plan's re-ordered CSR --
+// with U = 8 independent 16-byte B loads in flight per lane, flushing a row's
+// accumulators to C[perm[row]] whenever the stream crosses a row end. Short
+// rows thus cost no dependent load chain per row, and a launch keeps
+// thousands of items in flight.
+constexpr int kMaxCcJobs = 32;
+
+struct CcJob {
+    const int2 *items;
+    const int *perm, *p_row_ptr, *p_col;
+    const __half *p_val;
+    const __half *B;
+    void *C;
+    int n_items;
+    int M, K, N, ldb, ldc;
+    float alpha, beta;
+    unsigned flags;
+};
+
+struct CcBatch {
+    int n_jobs;
+    int block_start[kMaxCcJobs + 1];
+    CcJob job[kMaxCcJobs];
+};
+
+template <typename OutT, int L, bool VEC>
+__global__ void __launch_bounds__(256) spmm_cc_items_kernel(const __grid_constant__ CcBatch b)
+{
+    constexpr int G = 256 / L;      // groups per block
+    constexpr int W = VEC ? 8 : 1;  // output columns per lane per pass
+    constexpr int U = 8;            // B loads in flight per lane
+    __shared__ int s_rs[G][kItemRows + 1];
+    __shared__ int s_out[G][kItemRows];
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & (L - 1);
+    const int g = (int)threadIdx.x / L;
+    const unsigned gmask = (L == 32) ? 0xffffffffu : (((1u << L) - 1u) << (lane & ~(L - 1)));
+    int j = 0;
+    while (j + 1 < b.n_jobs && b.block_start[j + 1] <= (int)blockIdx.x) j++;
+    const CcJob &a = b.job[j];
+    const int item = ((int)blockIdx.x - b.block_start[j]) * G + g;
+    if (item >= a.n_items)
+        return; // whole group
+    const int2 it = a.items[item];
+    const int r0 = it.x, nrows = it.y - it.x;
+    for (int k = sub; k <= nrows; k += L) {
+        s_rs[g][k] = a.p_row_ptr[r0 + k];
+        if (k < nrows)
+            s_out[g][k] = a.perm[r0 + k];
+    }
+    __syncwarp(gmask);
+    const int j0 = s_rs[g][0], j1 = s_rs[g][nrows];
+    const bool keep = (a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) != 0;
+
+    for (int nb = 0; nb < a.N; nb += L * W) {
+        const int n0 = nb + sub * W;
+        const bool active = n0 < a.N;
+        float acc[W];
+#pragma unroll
+        for (int i = 0; i < W; i++) acc[i] = 0.f;
+        int cr = 0;
+        int ce = s_rs[g][1];
+        auto flush = [&]() {
+            const bool empty_row = s_rs[g][cr] == ce;
+            if (active && !(keep && empty_row)) {
+                OutT *cp = reinterpret_cast<OutT *>(a.C) + (size_t)s_out[g][cr] * a.ldc + n0;
+                float out[W];
+                if (a.beta != 0.f) {
+                    float old[W];
+                    if constexpr (VEC) load8(cp, old); else old[0] = to_f<OutT>(*cp);
+#pragma unroll
+                    for (int i = 0; i < W; i++) out[i] = fmaf(a.alpha, acc[i], a.beta * old[i]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < W; i++) out[i] = a.alpha * acc[i];
+                }
+                if constexpr (VEC) store8(cp, out); else *cp = from_f<OutT>(out[0]);
+            }
+#pragma unroll
+            for (int i = 0; i < W; i++) acc[i] = 0.f;
+            cr++;
+            ce = (cr < nrows) ? s_rs[g][cr + 1] : 0x7fffffff;
+        };
+        const __half *Bn = a.B + (active ? n0 : 0);
+        for (int base = j0; base < j1; base += L) {
+            const int jj = base + sub;
+            int c = -1;
+            float v = 0.f;
+            if (jj < j1) {
+                c = __ldg(a.p_col + jj);
+                v = __half2float(a.p_val[jj]);
+            }
+            const int cnt = min(L, j1 - base);
+            for (int t = 0; t < cnt; t += U) {
+                uint4 bv[U];
+                float av[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int cu = __shfl_sync(gmask, c, (t + u) & (L - 1), L);
+                    av[u] = __shfl_sync(gmask, v, (t + u) & (L - 1), L);
+                    bv[u] = make_uint4(0, 0, 0, 0);
+                    if (active && t + u < cnt) {
+                        if constexpr (VEC)
+                            bv[u] = __ldg(reinterpret_cast<const uint4 *>(Bn + (size_t)cu * a.ldb));
+                        else
+                            bv[u].x = __half_as_ushort(Bn[(size_t)cu * a.ldb]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (t + u < cnt) { // uniform across the group
+                        while (base + t + u >= ce) flush();
+                        if constexpr (VEC) {
+                            fma8(acc, av[u], bv[u]);
+                        } else {
+                            acc[0] = fmaf(av[u], __half2float(__ushort_as_half((unsigned short)bv[u].x)), acc[0]);
+                        }
+                    }
+                }
+            }
+        }
+        while (cr < nrows) flush();
+    }
+}
+
+template <typename OutT, int LPR>
+void launch_vec(const int *rp, const int *ci, const __half *v, int M, int K, int nnz, const __half *B, int ldb,
+                int N, OutT *C, int ldc, float alpha, float beta, unsigned flags, cudaStream_t s)
+{
+    const long long threads = (long long)M * LPR;
+    const unsigned grid = (unsigned)((threads + 255) / 256);
+    spmm_csr_vec_kernel<OutT, LPR><<<grid, 256, 0, s>>>(rp, ci, v, M, K, nnz, B, ldb, N, C, ldc, alpha, beta, flags);
+}
+
+inline int pick_lpr(int N) { return N <= 32 ? 4 : N <= 64 ? 8 : N <= 128 ? 16 : 32; }
+
+template <typename OutT>
+void dispatch_vec(const int *rp, const int *ci, const __half *v, int M, int K, int nnz, const __half *B, int ldb,
+                  int N, OutT *C, int ldc, float alpha, float beta, unsigned flags, cudaStream_t s)
+{
+    switch (pick_lpr(N)) {
+    case 4: launch_vec<OutT, 4>(rp, ci, v, M, K, nnz, B, ldb, N, C, ldc, alpha, beta, flags, s); break;
+    case 8: launch_vec<OutT, 8>(rp, ci, v, M, K, nnz, B, ldb, N, C, ldc, alpha, beta, flags, s); break;
+    case 16: launch_vec<OutT, 16>(rp, ci, v, M, K, nnz, B, ldb, N, C, ldc, alpha, beta, flags, s); break;
+    default: launch_vec<OutT, 32>(rp, ci, v, M, K, nnz, B, ldb, N, C, ldc, alpha, beta, flags, s); break;
+    }
+}
+
+bool vec_ok(const void *B, int ldb, int N, const void *C, int ldc, int c_dtype)
+{
+    const size_t c_elem = (c_dtype == TCA_DTYPE_F16) ? 2 : 4;
+    return (N % 8 == 0) && (ldb % 8 == 0) && aligned16(B) && aligned16(C) && ((ldc * c_elem) % 16 == 0);
+}
+
+} // namespace
+
+int launch_spmm_csr_cc(const int *row_ptr, const int *col_idx, const __half *vals, int M, int K, int nnz,
+                       const __half *B, int ldb, int N, void *C, int ldc, int c_dtype,
+                       float alpha, float beta, unsigned flags, cudaStream_t stream)
+{
+    if (vec_ok(B, ldb, N, C, ldc, c_dtype)) {
+        if (c_dtype == TCA_DTYPE_F16)
+            dispatch_vec<__half>(row_ptr, col_idx, vals, M, K, nnz, B, ldb, N, (__half *)C, ldc, alpha, beta, flags, stream);
+        else
+            dispatch_vec<float>(row_ptr, col_idx, vals, M, K, nnz, B, ldb, N, (float *)C, ldc, alpha, beta, flags, stream);
+    } else {
+        const unsigned grid = (unsigned)(((long long)M * 32 + 255) / 256);
+        if (c_dtype == TCA_DTYPE_F16)
+            spmm_csr_scalar_kernel<__half><<<grid, 256, 0, stream>>>(row_ptr, col_idx, vals, M, K, nnz, B, ldb, N,
+                                                                     (__half *)C, ldc, alpha, beta, flags);
+        else
+            spmm_csr_scalar_kernel<float><<<grid, 256, 0, stream>>>(row_ptr, col_idx, vals, M, K, nnz, B, ldb, N,
+                                                                    (float *)C, ldc, alpha, beta, flags);
+    }
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
+bool dense_operands_vec_ok(const void *B, int ldb, int N, const void *C, int ldc, int c_dtype)
+{
+    return vec_ok(B, ldb, N, C, ldc, c_dtype);
+}
+
+namespace {
+
+template <typename OutT, int LPR, bool VEC>
+int launch_cc_group(const CcBatch &b, cudaStream_t s)
+{
+    if (b.n_jobs == 0 || b.block_start[b.n_jobs] == 0)
+        return TCA_OK;
+    spmm_cc_items_kernel<OutT, LPR, VEC><<<b.block_start[b.n_jobs], 256, 0, s>>>(b);
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
+template <typename OutT>
+int launch_cc_typed(const CcBatch &b, int lpr, bool vec, cudaStream_t s)
+{
+    if (!vec) return launch_cc_group<OutT, 32, false>(b, s);
+    switch (lpr) {
+    case 4: return launch_cc_group<OutT, 4, true>(b, s);
+    case 8: return launch_cc_group<OutT, 8, true>(b, s);
+    case 16: return launch_cc_group<OutT, 16, true>(b, s);
+    default: return launch_cc_group<OutT, 32, true>(b, s);
+    }
+}
+
+} // namespace
+
+int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
+                   cudaStream_t s)
+{
+    // groups: (lanes per row, vectorised) -- 4/8/16/32 x vec, plus scalar
+    const int kinds[5][2] = {{4, 1}, {8, 1}, {16, 1}, {32, 1}, {32, 0}};
+    for (const auto &kd : kinds) {
+        CcBatch b;
+        b.n_jobs = 0;
+        b.block_start[0] = 0;
+        auto flush = [&]() -> int {
+            const int st = (c_dtype == TCA_DTYPE_F16) ? launch_cc_typed<__half>(b, kd[0], kd[1] != 0, s)
+                                                      : launch_cc_typed<float>(b, kd[0], kd[1] != 0, s);
+            b.n_jobs = 0;
+            return st;
+        };
+        for (int i = 0; i < n_jobs; i++) {
+            const SpmmJob &sj = jobs[i];
+            const tca_plan *p = sj.p;
+            const int n_items = sj.tc ? p->n_cc_items : p->n_all_items;
+            if (n_items == 0 || sj.N <= 0)
+                continue;
+            const bool vec = vec_ok(sj.B, sj.ldb, sj.N, sj.C, sj.ldc, c_dtype);
+            const int lpr = vec ? pick_lpr(sj.N) : 32;
+            if (lpr != kd[0] || (vec ? 1 : 0) != kd[1])
+                continue;
+            CcJob &a = b.job[b.n_jobs];
+            a.items = sj.tc ? p->cc_items : p->all_items;
+            a.perm = p->perm;
+            a.p_row_ptr = p->p_row_ptr;
+            a.p_col = p->p_col;
+            a.p_val = p->p_val;
+            a.B = sj.B;
+            a.C = sj.C;
+            a.n_items = n_items;
+            a.M = p->M;
+            a.K = p->K;
+            a.N = sj.N;
+            a.ldb = sj.ldb;
+            a.ldc = sj.ldc;
+            a.alpha = alpha;
+            a.beta = beta;
+            a.flags = flags;
+            const int per_block = 256 / lpr;
+            b.block_start[b.n_jobs + 1] = b.block_start[b.n_jobs] + (a.n_items + per_block - 1) / per_block;
+            b.n_jobs++;
+            if (b.n_jobs == kMaxCcJobs)
+                TCA_TRY(flush());
+        }
+        TCA_TRY(flush());
+    }
+    return TCA_OK;
+}
+
+} // namespace tca

@@ -1,0 +1,315 @@
+"""Python bindings of libtca_spmm.so (the B200 TCA-SpMM library).
+
+The library is called through its C ABI (include/tca_spmm.h) with ctypes;
+torch is used only to own device memory and streams. Nothing here computes
+on the CPU: when the shared library is missing the import of any compute
+function raises, so a missing build can never be masked by a fallback.
+
+Reference counterparts (paths within the reference project):
+  spmm / Plan.spmm     kernel_our_spmm_balanced   src/our_spmm.cu:290-346
+  Plan                 workload_manager           src/our_spmm.cu:347-471
+  spmm_host            our_spmm_balanced          src/our_spmm.cu:472-588
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+
+import numpy as np
+
+_PKG_ROOT = pathlib.Path(__file__).resolve().parents[2]
+LIB_PATH = pathlib.Path(os.environ.get("TCA_SPMM_LIB", _PKG_ROOT / "lib" / "libtca_spmm.so"))
+
+DTYPE_F16, DTYPE_F32, DTYPE_E4M3 = 0, 1, 2
+FLAG_KEEP_EMPTY_ROWS = 1
+
+# tca_plan_array_t
+ARR_ROW_PERM, ARR_P_ROW_PTR, ARR_P_COL, ARR_P_VAL, ARR_SRC = 0, 1, 2, 3, 4
+ARR_TC_WINDOWS, ARR_CC_WINDOWS, ARR_TILE_FIRST, ARR_WIN_COLS = 5, 6, 7, 8
+ARR_TILE_PTR, ARR_TILE_ENTRIES, ARR_TILE_SRC = 9, 10, 11
+ARR_TILE_IMAGE_IDX, ARR_TILE_IMAGES = 12, 13
+ARR_CC_ITEMS, ARR_ALL_ITEMS = 14, 15
+_ARR_DTYPE = {ARR_P_VAL: np.uint16, ARR_TILE_ENTRIES: np.uint32, ARR_TILE_IMAGES: np.uint16}
+
+STATUS = {
+    0: "TCA_OK", 1: "TCA_ERR_INVALID_ARG", 2: "TCA_ERR_CUDA", 3: "TCA_ERR_ALLOC",
+    4: "TCA_ERR_UNSUPPORTED", 5: "TCA_ERR_TIMEOUT", 6: "TCA_ERR_FORMAT", 7: "TCA_ERR_IO",
+}
+
+
+class TcaError(RuntimeError):
+    """A libtca_spmm entry point returned a non-zero tca_status_t."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class PlanOpts(ctypes.Structure):
+    _fields_ = [("sort_rows", ctypes.c_int), ("tc_min_density", ctypes.c_float),
+                ("path", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("M", ctypes.c_int), ("K", ctypes.c_int), ("nnz", ctypes.c_int),
+                ("n_windows", ctypes.c_int), ("n_tc_windows", ctypes.c_int),
+                ("n_cc_windows", ctypes.c_int), ("n_tc_chunks", ctypes.c_int),
+                ("n_images", ctypes.c_int), ("tc_nnz", ctypes.c_longlong),
+                ("format_bytes", ctypes.c_longlong)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class BatchItem(ctypes.Structure):
+    _fields_ = [("plan", ctypes.c_void_p), ("d_B_f16", ctypes.c_void_p), ("ldb", ctypes.c_int),
+                ("N", ctypes.c_int), ("d_C", ctypes.c_void_p), ("ldc", ctypes.c_int), ("n_tile", ctypes.c_int)]
+
+
+_lib = None
+
+_P, _I, _F, _U, _VP = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_uint, ctypes.c_void_p
+_SIGS = {
+    "tca_version": ([], ctypes.c_char_p),
+    "tca_last_error_string": ([], ctypes.c_char_p),
+    "tca_status_string": ([_I], ctypes.c_char_p),
+    "tca_spmm_csr": ([_P, _P, _P, _I, _I, _I, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP], _I),
+    "tca_plan_opts_default": ([ctypes.POINTER(PlanOpts)], None),
+    "tca_plan_create": ([_P, _P, _P, _I, _I, _I, ctypes.POINTER(PlanOpts), _VP, ctypes.POINTER(_VP)], _I),
+    "tca_plan_update_values": ([_VP, _P, _VP], _I),
+    "tca_plan_info": ([_VP, ctypes.POINTER(PlanInfo)], _I),
+    "tca_plan_export": ([_VP, _I, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], _I),
+    "tca_plan_status": ([_VP], _I),
+    "tca_plan_destroy": ([_VP], _I),
+    "tca_spmm": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP], _I),
+    "tca_spmm_events": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP, ctypes.POINTER(_VP)], _I),
+    "tca_plan_launch_counts": ([_VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
+    "tca_spmm_batched": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _VP, ctypes.POINTER(_VP)], _I),
+    "tca_spmm_host": ([_P, _P, _P, _I, _I, _I, _P, _I, _P, _I, _U, _I, ctypes.POINTER(ctypes.c_double)], _I),
+}
+
+
+def exported_symbols() -> list[str]:
+    """Names of the C-ABI entry points this module binds."""
+    return list(_SIGS)
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libtca_spmm.so once; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C tca-spmm_b200` "
+                               "(or __graft_entry__.build()); there is no CPU fallback")
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(handle, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = handle
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise TcaError(rc, lib().tca_last_error_string().decode())
+
+
+def version() -> str:
+    return lib().tca_version().decode()
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_handle(stream=None) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _ptr(t) -> int:
+    return t.data_ptr() if t is not None and t.numel() > 0 else 0
+
+
+def _out_code(dtype) -> int:
+    torch = _torch()
+    if dtype == torch.float16:
+        return DTYPE_F16
+    if dtype == torch.float32:
+        return DTYPE_F32
+    raise ValueError(f"output dtype {dtype} is not float16 or float32")
+
+
+def _check_dev(name, t, dtype):
+    torch = _torch()
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    del torch
+
+
+def _prepare_dense(B, out, M, out_dtype):
+    torch = _torch()
+    if B.dim() != 2 or B.dtype != torch.float16 or not B.is_cuda or B.stride(1) != 1:
+        raise ValueError("B must be a 2-D CUDA float16 tensor with unit column stride")
+    N = B.shape[1]
+    if out is None:
+        out = torch.empty((M, N), dtype=out_dtype, device=B.device)
+    if out.dim() != 2 or out.shape[0] != M or out.shape[1] != N or out.stride(1) != 1 or not out.is_cuda:
+        raise ValueError("out must be a CUDA M x N tensor with unit column stride")
+    return N, out
+
+
+def spmm_csr(row_ptr, col_idx, vals, B, K=None, out=None, out_dtype=None, alpha=1.0, beta=0.0,
+             keep_empty_rows=False, stream=None):
+    """Plan-free CUDA-core forward: out = alpha * A @ B + beta * out (tca_spmm_csr)."""
+    torch = _torch()
+    _check_dev("row_ptr", row_ptr, torch.int32)
+    _check_dev("col_idx", col_idx, torch.int32)
+    _check_dev("vals", vals, torch.float16)
+    M = row_ptr.numel() - 1
+    K = B.shape[0] if K is None else K
+    out_dtype = out_dtype or (out.dtype if out is not None else torch.float16)
+    N, out = _prepare_dense(B, out, M, out_dtype)
+    flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+    _check(lib().tca_spmm_csr(_ptr(row_ptr), _ptr(col_idx), _ptr(vals), M, K, vals.numel(),
+                              _ptr(B), B.stride(0), N, _ptr(out), out.stride(0), _out_code(out.dtype),
+                              alpha, beta, flags, _stream_handle(stream)))
+    return out
+
+
+PATHS = {"auto": 0, "cuda_core": 1, "tensor_core": 2}
+
+
+class Plan:
+    """The row-window, column-condensed tile format of one sparsity pattern,
+    built on the GPU by tca_plan_create (replaces workload_manager,
+    src/our_spmm.cu:347-471)."""
+
+    def __init__(self, row_ptr, col_idx, vals, K, sort_rows=True, tc_min_density=None,
+                 path="auto", stream=None):
+        torch = _torch()
+        _check_dev("row_ptr", row_ptr, torch.int32)
+        _check_dev("col_idx", col_idx, torch.int32)
+        _check_dev("vals", vals, torch.float16)
+        self._lib = lib()
+        opts = PlanOpts()
+        self._lib.tca_plan_opts_default(ctypes.byref(opts))
+        opts.sort_rows = 1 if sort_rows else 0
+        if tc_min_density is not None:
+            opts.tc_min_density = float(tc_min_density)
+        opts.path = PATHS[path]
+        self.M = row_ptr.numel() - 1
+        self.K = int(K)
+        self.nnz = col_idx.numel()
+        h = _VP()
+        _check(self._lib.tca_plan_create(_ptr(row_ptr), _ptr(col_idx), _ptr(vals), self.M, self.K,
+                                         self.nnz, ctypes.byref(opts), _stream_handle(stream),
+                                         ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        inf = PlanInfo()
+        _check(self._lib.tca_plan_info(self._h, ctypes.byref(inf)))
+        return inf.as_dict()
+
+    def export(self, which: int) -> np.ndarray:
+        n = ctypes.c_size_t()
+        _check(self._lib.tca_plan_export(self._h, which, None, 0, ctypes.byref(n)))
+        dt = _ARR_DTYPE.get(which, np.int32)
+        arr = np.empty(n.value // np.dtype(dt).itemsize, dtype=dt)
+        if n.value:
+            _check(self._lib.tca_plan_export(self._h, which, arr.ctypes.data, n.value, ctypes.byref(n)))
+        return arr
+
+    def update_values(self, vals, stream=None):
+        _check(self._lib.tca_plan_update_values(self._h, _ptr(vals), _stream_handle(stream)))
+
+    def status(self):
+        _check(self._lib.tca_plan_status(self._h))
+
+    def spmm(self, B, out=None, out_dtype=None, alpha=1.0, beta=0.0, keep_empty_rows=False, stream=None):
+        """out = alpha * A @ B + beta * out through the plan (tca_spmm)."""
+        torch = _torch()
+        out_dtype = out_dtype or (out.dtype if out is not None else torch.float16)
+        N, out = _prepare_dense(B, out, self.M, out_dtype)
+        flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+        _check(self._lib.tca_spmm(self._h, _ptr(B), B.stride(0), N, _ptr(out), out.stride(0),
+                                  _out_code(out.dtype), alpha, beta, flags, _stream_handle(stream)))
+        return out
+
+    def spmm_events(self, B, out, events, alpha=1.0, beta=0.0, keep_empty_rows=False, stream=None):
+        """Plan.spmm recording 4 torch.cuda.Event objects (or None) around the
+        tensor-core and CUDA-core kernels (tca_spmm_events)."""
+        N, out = _prepare_dense(B, out, self.M, out.dtype)
+        arr = (_VP * 4)(*[(e.cuda_event if e is not None else None) for e in events])
+        flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+        _check(self._lib.tca_spmm_events(self._h, _ptr(B), B.stride(0), N, _ptr(out), out.stride(0),
+                                         _out_code(out.dtype), alpha, beta, flags, _stream_handle(stream), arr))
+        return out
+
+    def launch_counts(self, N: int) -> tuple[int, int]:
+        a, b = _I(), _I()
+        _check(self._lib.tca_plan_launch_counts(self._h, N, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.tca_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def spmm_batched(plans, Bs, outs, alpha=1.0, beta=0.0, keep_empty_rows=False, n_tile=0, events=None,
+                 stream=None):
+    """Forwards of many plans in a few launches (tca_spmm_batched). `outs`
+    must all have the same dtype (float16 or float32)."""
+    n = len(plans)
+    arr = (BatchItem * max(n, 1))()
+    for i, (p, B, C) in enumerate(zip(plans, Bs, outs)):
+        N, _ = _prepare_dense(B, C, p.M, C.dtype)
+        arr[i] = BatchItem(p.handle, _ptr(B), B.stride(0), N, _ptr(C), C.stride(0), n_tile)
+    code = _out_code(outs[0].dtype) if n else DTYPE_F16
+    ev = None
+    if events is not None:
+        ev = (_VP * 4)(*[(e.cuda_event if e is not None else None) for e in events])
+    flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+    _check(lib().tca_spmm_batched(arr, n, code, alpha, beta, flags, _stream_handle(stream), ev))
+    return outs
+
+
+def spmm_host(row_ptr: np.ndarray, col_idx: np.ndarray, vals: np.ndarray, K: int, B: np.ndarray,
+              C: np.ndarray | None = None, keep_empty_rows=True, n_iter=1):
+    """Host-buffer forward with the reference's convention (tca_spmm_host ->
+    our_spmm_balanced semantics): numpy in, numpy out, C float32 or float16.
+    Returns (C, mean device ms of one forward)."""
+    M = row_ptr.size - 1
+    N = B.shape[1]
+    if C is None:
+        C = np.zeros((M, N), dtype=np.float32)
+    code = DTYPE_F32 if C.dtype == np.float32 else DTYPE_F16
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_idx, dtype=np.int32)
+    v = np.ascontiguousarray(vals, dtype=np.float16)
+    Bc = np.ascontiguousarray(B, dtype=np.float16)
+    ms = ctypes.c_double()
+    flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+    _check(lib().tca_spmm_host(rp.ctypes.data, ci.ctypes.data, v.ctypes.data, M, K, ci.size,
+                               Bc.ctypes.data, N, C.ctypes.data, code, flags, n_iter, ctypes.byref(ms)))
+    return C, ms.value

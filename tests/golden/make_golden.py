@@ -1,0 +1,105 @@
+"""Generates the golden fixtures in this directory by running the reference's
+own CPU functions, compiled from the reference sources into
+oracle/_ref/libtcaref.so (`make -C oracle ref`):
+
+  smtx_*.smtx            seeded synthetic smtx files (written by this script)
+  golden.npz             for each case, the reference's outputs:
+    smtx_<i>_coords      smtx_input_to_Dense (src/file_input.cu:135-193) on
+                         smtx_<i>.smtx, stored as the (row, col) pairs of its
+                         nonzeros (all values are 1.0) plus the shape
+    d2c_<i>_*            convert_dense_to_csr (src/miscalleneous.cu:29-65) on a
+                         seeded dense FP16 matrix with -0.0, subnormals and
+                         repeated values
+    c2d_<i>_dense        convert_csr_to_dense (src/miscalleneous.cu:66-81)
+    gemm_<i>_*           naive_gemm (src/miscalleneous.cu:114-134) on a seeded
+                         sparse A (dense storage) and B
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import pathlib
+import subprocess
+import sys
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from oracle import oracle  # noqa: E402
+
+OUT = pathlib.Path(__file__).resolve().parent
+
+
+def write_smtx(path, M, K, row_ptr, col):
+    """Same layout as the reference fixture: header, row_ptr line, col line,
+    single spaces with a trailing space."""
+    with open(path, "w") as f:
+        f.write(f"{M}, {K}, {int(row_ptr[-1])}\n")
+        f.write("".join(f"{x} " for x in row_ptr) + "\n")
+        f.write("".join(f"{x} " for x in col) + "\n")
+
+
+def smtx_cases(rng):
+    cases = []
+    # mostly-empty rows with one row above 64 nnz (both reference kernel paths)
+    M, K = 2048, 512
+    nz_rows = rng.choice(M, 28, replace=False)
+    row_nnz = np.zeros(M, np.int64)
+    row_nnz[nz_rows] = rng.integers(1, 60, size=28)
+    row_nnz[nz_rows[0]] = 65
+    cases.append((M, K, row_nnz))
+    # small dense-ish and ragged cases
+    cases.append((37, 53, rng.binomial(53, 0.3, size=37)))
+    cases.append((64, 1024, np.where(rng.random(64) < 0.2, 0, rng.integers(1, 1024, size=64))))
+    out = []
+    for M, K, row_nnz in cases:
+        row_ptr = np.zeros(M + 1, np.int32)
+        np.cumsum(row_nnz, out=row_ptr[1:])
+        cols = [np.sort(rng.choice(K, int(n), replace=False)) for n in row_nnz]
+        col = np.concatenate(cols).astype(np.int32) if cols else np.zeros(0, np.int32)
+        out.append((M, K, row_ptr, col))
+    return out
+
+
+def dense_case(rng, M, K, density):
+    A = (rng.standard_normal((M, K)) * 0.5).astype(np.float16)
+    A[rng.random((M, K)) >= density] = 0
+    bits = A.view(np.uint16)
+    neg0 = rng.random((M, K)) < 0.02
+    bits[neg0] = 0x8000                       # -0.0 is not a nonzero
+    sub = rng.random((M, K)) < 0.01
+    bits[sub] = rng.integers(1, 0x3ff, size=int(sub.sum()), dtype=np.uint16)  # subnormals are
+    return A
+
+
+def main():
+    subprocess.run(["make", "-C", str(ROOT / "oracle"), "all", "ref"], check=True)
+    rng = np.random.default_rng(20240601)
+    g = {}
+    for i, (M, K, row_ptr, col) in enumerate(smtx_cases(rng)):
+        path = OUT / f"smtx_{i}.smtx"
+        write_smtx(path, M, K, row_ptr, col)
+        A, nnz = oracle.ref_smtx_to_dense(path)
+        r, c = np.nonzero(A.view(np.uint16))
+        assert np.all(A[r, c] == 1.0)
+        g[f"smtx_{i}_shape"] = np.array([A.shape[0], A.shape[1], nnz], np.int64)
+        g[f"smtx_{i}_coords"] = np.stack([r, c]).astype(np.int32)
+    for i, (M, K, d) in enumerate([(33, 47, 0.3), (128, 64, 0.05), (7, 300, 0.6)]):
+        A = dense_case(rng, M, K, d)
+        rp, ci, v = oracle.ref_dense_to_csr(A)
+        g[f"d2c_{i}_A"] = A
+        g[f"d2c_{i}_row_ptr"], g[f"d2c_{i}_col"], g[f"d2c_{i}_val"] = rp, ci, v
+        g[f"c2d_{i}_dense"] = oracle.ref_csr_to_dense(M, K, rp, ci, v)
+    for i, (M, K, N, d) in enumerate([(64, 96, 40, 0.2), (128, 256, 64, 0.05), (30, 70, 24, 0.9)]):
+        A = (rng.standard_normal((M, K)) * 0.3).astype(np.float16)
+        A[rng.random((M, K)) >= d] = 0
+        B = rng.uniform(-1, 1, size=(K, N)).astype(np.float16)
+        g[f"gemm_{i}_A"], g[f"gemm_{i}_B"] = A, B
+        g[f"gemm_{i}_C"] = oracle.ref_naive_gemm(A, B)
+    np.savez_compressed(OUT / "golden.npz", **g)
+    print("wrote", OUT / "golden.npz", len(g), "arrays")
+
+
+if __name__ == "__main__":
+    main()
