@@ -436,7 +436,7 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
     int tc_possible = (path != 1) && K <= MAX_TC_K && K > 0;
     int *rank = (int *)malloc(sizeof(int) * (K > 0 ? K : 1));
     int *is_tc = (int *)calloc((size_t)W, sizeof(int)), *nch = (int *)calloc((size_t)W, sizeof(int));
-    int *wnnz = (int *)calloc((size_t)W, sizeof(int));
+    int *wnnz = (int *)calloc((size_t)W, sizeof(int)), *direct = (int *)calloc((size_t)W, sizeof(int));
     for (int w = 0; w < W; w++) {
         int r0 = w * WR, r1 = r0 + WR < M ? r0 + WR : M;
         int lo = p->p_row_ptr[r0], hi = p->p_row_ptr[r1];
@@ -446,9 +446,18 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
         for (int i = r0; i < r1; i++) elig &= row_sorted[p->perm[i]];
         for (int c = 0; c < K; c++) rank[c] = 0;
         for (int j = lo; j < hi; j++) rank[p->p_col[j]] = 1;
-        int nu = 0;
+        int nu = 0, nblk = 0;
         for (int c = 0; c < K; c++) nu += rank[c];
-        nch[w] = (nu + CW - 1) / CW;
+        for (int b = 0; b * CW < K; b++) {
+            int hit = 0;
+            for (int c = b * CW; c < (b + 1) * CW && c < K; c++) hit |= rank[c];
+            nblk += hit;
+        }
+        /* direct chunks (the touched 64-column blocks of K) when they need at
+         * most twice the chunks of the condensed distinct columns */
+        int nch_cond = (nu + CW - 1) / CW;
+        direct[w] = nblk <= 2 * nch_cond;
+        nch[w] = direct[w] ? nblk : nch_cond;
         if (elig && wnnz[w] > 0) {
             if (path == 2) is_tc[w] = 1;
             else is_tc[w] = (double)wnnz[w] >= (double)tc_min_density * (double)(WR * CW) * (double)nch[w];
@@ -479,6 +488,12 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
         int r0 = w * WR, r1 = r0 + WR < M ? r0 + WR : M;
         for (int c = 0; c < K; c++) rank[c] = 0;
         for (int j = p->p_row_ptr[r0]; j < p->p_row_ptr[r1]; j++) rank[p->p_col[j]] = 1;
+        if (direct[w])
+            for (int b = 0; b * CW < K; b++) {
+                int hit = 0;
+                for (int c = b * CW; c < (b + 1) * CW && c < K; c++) hit |= rank[c];
+                for (int c = b * CW; c < (b + 1) * CW && c < K; c++) rank[c] = hit;
+            }
         int nu = 0;
         for (int c = 0; c < K; c++) {
             if (rank[c]) { p->win_cols[(size_t)c0 * CW + nu] = c; rank[c] = nu++; }
@@ -502,13 +517,13 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
         }
         p->tile_ptr[c0 + nch[w]] = (int)base;
     }
-    /* chunks with >= 4096 entries also become a dense 128 x 64 FP16 tile in
+    /* chunks with >= 2048 entries also become a dense 128 x 64 FP16 tile in
      * the 128-byte swizzled K-major layout: element (r, c) at byte
      * r*128 + ((c/8) ^ (r%8))*16 + (c%8)*2 */
     p->img_idx = (int *)malloc(sizeof(int) * ((size_t)p->n_tc_chunks + 1));
     p->n_images = 0;
     for (int c = 0; c < p->n_tc_chunks; c++)
-        p->img_idx[c] = (p->tile_ptr[c + 1] - p->tile_ptr[c] >= WR * CW / 2) ? p->n_images++ : -1;
+        p->img_idx[c] = (p->tile_ptr[c + 1] - p->tile_ptr[c] >= WR * CW / 4) ? p->n_images++ : -1;
     p->images = (uint16_t *)calloc((size_t)p->n_images * WR * CW + 1, sizeof(uint16_t));
     for (int c = 0; c < p->n_tc_chunks; c++) {
         if (p->img_idx[c] < 0) continue;
@@ -528,6 +543,6 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
     p->all_items = (int *)malloc(sizeof(int) * (2 * (size_t)p->n_all_items + 1));
     orc_build_items(all, W, p->p_row_ptr, M, p->all_items);
     free(all);
-    free(cur); free(rank); free(is_tc); free(nch); free(wnnz); free(row_nnz); free(row_sorted);
+    free(cur); free(rank); free(is_tc); free(nch); free(wnnz); free(direct); free(row_nnz); free(row_sorted);
     return 0;
 }

@@ -96,14 +96,14 @@ __global__ void k_permute(const int *__restrict__ perm, const int *__restrict__ 
 // 3. Window statistics: one block per window, K-bit bitmap in shared memory.
 __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
                                const int *__restrict__ p_sorted, int M, int K, int *__restrict__ win_nu,
-                               int *__restrict__ win_nnz, int *__restrict__ win_elig)
+                               int *__restrict__ win_nnz, int *__restrict__ win_elig, int *__restrict__ win_nblk)
 {
     extern __shared__ uint32_t bm[];
-    __shared__ int s_cnt, s_elig;
+    __shared__ int s_cnt, s_elig, s_nblk;
     const int w = blockIdx.x;
     const int nwords = (K + 31) >> 5;
     for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
-    if (threadIdx.x == 0) { s_cnt = 0; s_elig = 1; }
+    if (threadIdx.x == 0) { s_cnt = 0; s_elig = 1; s_nblk = 0; }
     __syncthreads();
     const int r0 = w * kWindowRows, r1 = min(M, r0 + kWindowRows);
     const int lo = p_row_ptr[r0], hi = p_row_ptr[r1];
@@ -116,12 +116,17 @@ __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__r
     __syncthreads();
     int cnt = 0;
     for (int i = threadIdx.x; i < nwords; i += blockDim.x) cnt += __popc(bm[i]);
-    atomicAdd(&s_cnt, cnt); // integer sum: order-independent
+    atomicAdd(&s_cnt, cnt); // integer sums: order-independent
+    int nb = 0;
+    for (int b = threadIdx.x; 2 * b < nwords; b += blockDim.x)
+        nb += ((bm[2 * b] | (2 * b + 1 < nwords ? bm[2 * b + 1] : 0u)) != 0u);
+    atomicAdd(&s_nblk, nb);
     __syncthreads();
     if (threadIdx.x == 0) {
         win_nu[w] = s_cnt;
         win_nnz[w] = hi - lo;
         win_elig[w] = s_elig;
+        win_nblk[w] = s_nblk;
     }
 }
 
@@ -151,8 +156,8 @@ __device__ int block_exclusive_scan128(int v, int *total, int *scratch /* >= 5 i
 
 // 5. Tile fill: one block of 128 threads per tensor-core window.
 __global__ void __launch_bounds__(128)
-k_tile_fill(const int *__restrict__ tc_windows, const int *__restrict__ tile_first,
-            const long long *__restrict__ entry_base, const int *__restrict__ p_row_ptr,
+k_tile_fill(const int4 *__restrict__ win_info, const long long *__restrict__ entry_base,
+            const int *__restrict__ p_row_ptr,
             const int *__restrict__ p_col, const __half *__restrict__ p_val, int M, int K,
             int *__restrict__ win_cols, int *__restrict__ tile_ptr, uint32_t *__restrict__ entries,
             int *__restrict__ tile_src)
@@ -163,8 +168,8 @@ k_tile_fill(const int *__restrict__ tc_windows, const int *__restrict__ tile_fir
     uint32_t *bm = sm;
     int *pre = reinterpret_cast<int *>(sm + nwords);
     const int t = blockIdx.x;
-    const int w = tc_windows[t];
-    const int c0 = tile_first[t], nch = tile_first[t + 1] - c0;
+    const int4 wi = win_info[t];
+    const int w = wi.x, c0 = wi.y, nch = wi.z;
     const int r0 = w * kWindowRows, r1 = min(M, r0 + kWindowRows);
     const int lo = p_row_ptr[r0], hi = p_row_ptr[r1];
 
@@ -175,6 +180,17 @@ k_tile_fill(const int *__restrict__ tc_windows, const int *__restrict__ tile_fir
         atomicOr(&bm[c >> 5], 1u << (c & 31));
     }
     __syncthreads();
+    if (wi.w) { // direct window: every column < K of each touched 64-column block
+        for (int b = threadIdx.x; 2 * b < nwords; b += blockDim.x) {
+            const bool hit = (bm[2 * b] | (2 * b + 1 < nwords ? bm[2 * b + 1] : 0u)) != 0u;
+            for (int q = 0; q < 2 && 2 * b + q < nwords; q++) {
+                const int base = (2 * b + q) * 32;
+                const int valid = min(32, K - base);
+                bm[2 * b + q] = hit ? (valid >= 32 ? 0xffffffffu : ((1u << valid) - 1u)) : 0u;
+            }
+        }
+        __syncthreads();
+    }
     // exclusive prefix of popcounts over words: each thread owns a contiguous segment
     const int seg = (nwords + 127) / 128;
     const int wb = min(nwords, (int)threadIdx.x * seg), we = min(nwords, wb + seg);
@@ -286,7 +302,8 @@ void free_plan(tca_plan *p)
     if (!p) return;
     void *arrs[] = {p->perm, p->p_row_ptr, p->p_col, p->p_val, p->src, p->tc_windows, p->cc_windows,
                     p->all_windows, p->tile_first, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src,
-                    p->img_idx, p->images, p->img_chunk, p->cc_items, p->all_items, p->d_status};
+                    p->img_idx, p->images, p->img_chunk, p->cc_items, p->all_items, p->tc_win_info,
+                    p->d_status};
     for (void *a : arrs)
         if (a) cudaFree(a);
     delete p;
@@ -389,30 +406,38 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     TCA_TRY(dev_alloc(&p->all_windows, W, bytes));
     TCA_CUDA_TRY(cudaMemcpyAsync(p->all_windows, h_all.data(), sizeof(int) * W, cudaMemcpyHostToDevice, s));
 
-    std::vector<int> h_nu(W, 0), h_nnz(W, 0), h_elig(W, 0);
+    std::vector<int> h_nu(W, 0), h_nnz(W, 0), h_elig(W, 0), h_nblk(W, 0);
     const bool tc_possible = (p->opts.path != 1) && K <= kMaxTcK && K > 0 && W > 0;
     if (tc_possible) {
-        DevBuf t_nu, t_wn, t_el;
-        int *d_nu, *d_wn, *d_el;
+        DevBuf t_nu, t_wn, t_el, t_nb;
+        int *d_nu, *d_wn, *d_el, *d_nb;
+        TCA_TRY(dev_alloc(&d_nb, W, nullptr)); t_nb.p = d_nb;
         TCA_TRY(dev_alloc(&d_nu, W, nullptr)); t_nu.p = d_nu;
         TCA_TRY(dev_alloc(&d_wn, W, nullptr)); t_wn.p = d_wn;
         TCA_TRY(dev_alloc(&d_el, W, nullptr)); t_el.p = d_el;
         const size_t smem = sizeof(uint32_t) * ((K + 31) / 32);
         TCA_CUDA_TRY(cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_window_stats<<<W, 256, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, d_nu, d_wn, d_el);
+        k_window_stats<<<W, 256, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, d_nu, d_wn, d_el, d_nb);
         TCA_CUDA_TRY(cudaGetLastError());
         TCA_CUDA_TRY(cudaMemcpyAsync(h_nu.data(), d_nu, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
         TCA_CUDA_TRY(cudaMemcpyAsync(h_nnz.data(), d_wn, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
         TCA_CUDA_TRY(cudaMemcpyAsync(h_elig.data(), d_el, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
+        TCA_CUDA_TRY(cudaMemcpyAsync(h_nblk.data(), d_nb, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
         TCA_CUDA_TRY(cudaStreamSynchronize(s));
     }
 
     // 4. path decision (host, deterministic)
-    std::vector<int> tc_list, cc_list, h_first(1, 0);
+    // A window's chunks are "direct" (the 64-column blocks of K it touches,
+    // whose B rows are contiguous and load as tiled TMA boxes) when that needs
+    // at most twice the chunks of condensing its distinct columns (gathered
+    // B rows); otherwise condensed.
+    std::vector<int> tc_list, cc_list, h_first(1, 0), h_direct;
     std::vector<long long> h_ebase;
     long long ebase = 0;
     for (int w = 0; w < W; w++) {
-        const int nch = (h_nu[w] + kChunkCols - 1) / kChunkCols;
+        const int nch_cond = (h_nu[w] + kChunkCols - 1) / kChunkCols;
+        const bool direct = h_nblk[w] <= 2 * nch_cond;
+        const int nch = direct ? h_nblk[w] : nch_cond;
         bool tc = false;
         if (tc_possible && h_elig[w] && h_nnz[w] > 0) {
             if (p->opts.path == 2)
@@ -422,6 +447,7 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         }
         if (tc) {
             tc_list.push_back(w);
+            h_direct.push_back(direct ? 1 : 0);
             h_first.push_back(h_first.back() + nch);
             h_ebase.push_back(ebase);
             ebase += h_nnz[w];
@@ -441,6 +467,12 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     if (p->n_cc)
         TCA_CUDA_TRY(cudaMemcpyAsync(p->cc_windows, cc_list.data(), sizeof(int) * p->n_cc, cudaMemcpyHostToDevice, s));
     TCA_CUDA_TRY(cudaMemcpyAsync(p->tile_first, h_first.data(), sizeof(int) * (p->n_tc + 1), cudaMemcpyHostToDevice, s));
+    std::vector<int4> h_wi((size_t)p->n_tc);
+    for (int t = 0; t < p->n_tc; t++)
+        h_wi[t] = make_int4(tc_list[t], h_first[t], h_first[t + 1] - h_first[t], h_direct[t]);
+    TCA_TRY(dev_alloc(&p->tc_win_info, (size_t)p->n_tc, bytes));
+    if (p->n_tc)
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->tc_win_info, h_wi.data(), sizeof(int4) * p->n_tc, cudaMemcpyHostToDevice, s));
 
     // 5. tiles
     TCA_TRY(dev_alloc(&p->win_cols, (size_t)p->n_tc_chunks * kChunkCols, bytes));
@@ -455,7 +487,7 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         TCA_CUDA_TRY(cudaMemcpyAsync(d_eb, h_ebase.data(), sizeof(long long) * p->n_tc, cudaMemcpyHostToDevice, s));
         const size_t smem = 2 * sizeof(uint32_t) * ((K + 31) / 32);
         TCA_CUDA_TRY(cudaFuncSetAttribute(k_tile_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tile_fill<<<p->n_tc, 128, smem, s>>>(p->tc_windows, p->tile_first, d_eb, p->p_row_ptr, p->p_col, p->p_val,
+        k_tile_fill<<<p->n_tc, 128, smem, s>>>(p->tc_win_info, d_eb, p->p_row_ptr, p->p_col, p->p_val,
                                                M, K, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src);
         TCA_CUDA_TRY(cudaGetLastError());
         TCA_CUDA_TRY(cudaStreamSynchronize(s)); // d_eb is freed at scope exit
@@ -626,6 +658,8 @@ int tca_plan_status(tca_plan_t p)
     TCA_CUDA_TRY(cudaMemcpy(&h, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
     if (h & kStatusTimeout)
         return set_error(TCA_ERR_TIMEOUT, "a bounded device-side wait gave up (status word 0x%x)", h);
+    if (h & kStatusLayout)
+        return set_error(TCA_ERR_UNSUPPORTED, "tensor-core kernel skipped: shared memory base not 1024-byte aligned");
     return TCA_OK;
 }
 

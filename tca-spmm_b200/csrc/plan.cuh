@@ -18,8 +18,9 @@
 //                      tile_src indexes p_val; 4 zero entries of padding let
 //                      16-byte copies round the end of the last chunk up
 //   img_idx[chunks], images[n_images * 8192] (FP16)
-//                      chunks with >= 4096 nonzeros (half the tile: fewer
-//                      bytes as a dense tile than as entries) are also kept
+//                      chunks with >= 2048 nonzeros (a quarter of the tile:
+//                      at most twice the bytes of their entries, and no
+//                      scatter work) are also kept
 //                      as a dense 128 x 64 tile, already in the 128-byte
 //                      swizzled K-major layout the tensor cores read from
 //                      shared memory; img_idx is -1 for the other chunks
@@ -40,6 +41,7 @@ struct tca_plan {
     int *cc_windows = nullptr;
     int *all_windows = nullptr;
     int *tile_first = nullptr;
+    int4 *tc_win_info = nullptr; // per tensor-core window: {window, first chunk, chunk count, 0}
     int *win_cols = nullptr;
     int *tile_ptr = nullptr;
     uint32_t *tile_entries = nullptr;
@@ -61,7 +63,7 @@ struct tca_plan {
 
 namespace tca {
 
-constexpr int kImageMinNnz = kWindowRows * kChunkCols / 2; // 4096
+constexpr int kImageMinNnz = kWindowRows * kChunkCols / 4; // 2048
 constexpr int kEntryPad = 4;
 constexpr int kItemRows = 31;
 constexpr int kItemNnz = 32;
@@ -79,6 +81,7 @@ constexpr int kMaxTcK = 1 << 17;
 
 // Device status bits.
 constexpr int kStatusTimeout = 1;
+constexpr int kStatusLayout = 2; // shared memory base not 1024-byte aligned: the kernel did no work
 
 // One forward of one plan, as the batched launchers see it.
 struct SpmmJob {

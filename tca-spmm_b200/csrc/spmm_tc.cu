@@ -9,41 +9,50 @@
 // tile multiplies the 64 matching rows of B on the 5th-generation tensor
 // cores: D[128 x NT] (FP32, tensor memory) += A[128 x 64] * B[64 x NT].
 //
-// One CTA = one (job, window, NT-wide slice of N) work item; 5 warps:
-//   warps 0-3 (producers), per chunk:
-//     * dense chunks (>= 4096 nonzeros): one thread issues a 16 KB bulk copy
-//       (cp.async.bulk, complete_tx on the stage's "full" mbarrier) of the
-//       pre-rendered, pre-swizzled A tile straight into the stage;
-//     * sparse chunks: zero the A tile; copy the packed entries into a
-//       staging buffer with 16-byte cp.async; one chunk later, scatter them
-//       into the 128-byte swizzled K-major tile;
-//     * gather the 64 B rows (the chunk's condensed columns, preloaded in
-//       shared memory) into a 128-byte swizzled N-major tile with 16-byte
-//       cp.async, zero-filling padding columns and n >= N;
-//     * fence.proxy.async, then arrive on "full".
-//   warp 4, one lane: wait "full", issue 4 tcgen05.mma (K = 16 each),
-//     tcgen05.commit the stage's "empty" barrier; after the last chunk commit
-//     the "accumulator ready" barrier.
-//   warps 0-3 (epilogue): tcgen05.ld the accumulator (TMEM lane = row),
-//     alpha/beta, store to C[perm[row]] (FP16 or FP32).
+// One CTA = one (job, window, NT-wide slice of N) work item, a ring of
+// kStages (A tile, B tile, entry staging) stages and three decoupled roles:
+//   * one loader warp moves every byte through the TMA engine: the 64 B rows
+//     of the chunk's condensed columns by tile::gather4 (4 rows x 128 bytes
+//     per instruction into a 128-byte swizzled N-major tile; padding columns
+//     and n >= N are out of the tensor and arrive as zeros), and either the
+//     chunk's pre-rendered, pre-swizzled dense A tile (chunks with >= 2048
+//     nonzeros: one 16 KB cp.async.bulk) or its packed entries (cp.async.bulk
+//     into the stage's staging buffer);
+//   * scatter warps, once a stage's entries landed, zero its A tile and
+//     scatter them into the 128-byte swizzled K-major layout;
+//   * one MMA lane issues 4 tcgen05.mma (K = 16 each) per chunk into the FP32
+//     accumulator in tensor memory and releases the stage with tcgen05.commit;
+//   * finally 4 warps read the accumulator (TMEM lane = row) and store
+//     alpha * D + beta * C to C[perm[row]] (FP16 or FP32).
+// Per-thread 16-byte cp.async was measured to issue only ~13 B/clock/SM for
+// the B gather, which left the tensor cores idle; the TMA engine does not
+// occupy the issuing threads.
 // Every mbarrier wait is bounded (about one second of %globaltimer); on
 // expiry the CTA records kStatusTimeout in the job's status word and runs to
 // completion without hanging. No load uses cluster multicast.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <mutex>
 #include "tca_internal.cuh"
 #include "plan.cuh"
 
 namespace tca {
 namespace {
 
-constexpr int kProducerThreads = 128;
-constexpr int kThreads = kProducerThreads + 32;
-constexpr int kATileBytes = kWindowRows * kChunkCols * 2; // 16 KB
-constexpr int kStagingBytes = kImageMinNnz * 4 + 64;      // < 4096 entries, rounded out to 16 B
-constexpr int kMetaChunks = 32;                           // chunk metadata cached in shared memory
-constexpr int kMaxJobs = 32;                              // jobs per launch (kernel parameter space)
+constexpr int kScatterThreads = 128; // warps 0-3: scatter, then epilogue
+constexpr int kLoaderWarp = 4;       // TMA issue
+constexpr int kMmaWarp = 5;          // TMEM allocation, tcgen05.mma issue
+constexpr int kThreads = 192;
+constexpr int kATileBytes = kWindowRows * kChunkCols * 2;     // 16 KB
+constexpr int kStagingBytes = ((kImageMinNnz + 3) * 4 + 15) & ~15; // entries of a sparse chunk, 16-byte rounded
+constexpr int kMetaChunks = 8;                                // chunk metadata cached in shared memory
+constexpr int kMaxJobs = 32;                                  // jobs per launch (kernel parameter space)
 
 struct TcJob {
-    const int *tc_windows, *tile_first, *tile_ptr, *win_cols, *img_idx, *perm, *p_row_ptr;
+    CUtensorMap tmap_b;    // B as a 2-D tensor {N, K}, box {64, 1}, 128-byte swizzle (gather4 source)
+    CUtensorMap tmap_tile; // the same tensor, box {64, 64}: 64 contiguous rows of B per instruction
+    const int4 *win_info; // per tensor-core window: window, first chunk, chunk count
+    const int *tile_ptr, *win_cols, *img_idx, *perm, *p_row_ptr;
     const uint32_t *entries;
     const uint16_t *images;
     const __half *B;
@@ -111,12 +120,6 @@ __device__ __forceinline__ void named_bar_sync(int id, int n)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // 1-D bulk copy global -> this CTA's shared memory, completing on `bar`.
@@ -124,6 +127,35 @@ __device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uin
 {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// mbarrier arrive (count 1) that also adds `bytes` to the transaction count.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// TMA gather of 4 rows (y0..y3) x one 64-element box starting at column x of a
+// 2-D tensor into shared memory, completing on `bar`. Rows or columns outside
+// the tensor are zero-filled.
+__device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap *map, int x, int y0, int y1, int y2,
+                                            int y3, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(dst),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3)
+                 : "memory");
+}
+
+// TMA load of a {64 columns x 64 rows} box of a 2-D tensor at (x, y) into
+// shared memory, completing on `bar`; out-of-range elements are zero-filled.
+__device__ __forceinline__ void tma_tile2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
                  : "memory");
 }
 
@@ -203,38 +235,59 @@ __device__ __forceinline__ void store8_out(float *p, const float *v, float alpha
     reinterpret_cast<float4 *>(p)[1] = make_float4(o[4], o[5], o[6], o[7]);
 }
 
-// Shared memory: kStages x (A tile | B tile), kStages entry staging buffers,
-// chunk metadata, per-stage pending-chunk records, mbarriers.
+// Shared memory (1024-byte aligned base): kStages x (A tile | B tile),
+// kStages entry staging buffers, per-stage pending-chunk records, the loader's
+// chunk metadata cache, mbarriers (full, empty, staged per stage; accumulator
+// ready), two broadcast flags and the TMEM address slot.
 template <int NT> struct TcCfg {
-    static constexpr int kStages = NT == 256 ? 3 : 4;
+    static constexpr int kStages = NT == 256 ? 4 : NT == 128 ? 5 : 7;
     static constexpr int kBTileBytes = kChunkCols * NT * 2;
     static constexpr int kStage = kATileBytes + kBTileBytes;
     static constexpr int kStagingOff = kStages * kStage;
-    static constexpr int kMetaOff = kStagingOff + kStages * kStagingBytes;
+    static constexpr int kPendOff = kStagingOff + kStages * kStagingBytes;
+    static constexpr int kMetaOff = kPendOff + kStages * 16;
     static constexpr int kMetaBytes = (kMetaChunks * kChunkCols + 2 * kMetaChunks + 1) * 4;
-    static constexpr int kPendOff = kMetaOff + kMetaBytes;
-    static constexpr int kBarOff = (kPendOff + kStages * 16 + 15) & ~15;
-    static constexpr int kBytes = kBarOff + (2 * kStages + 1) * 8 + 16;
-    static constexpr int kSmem = kBytes + 1024; // alignment slack
+    static constexpr int kBarOff = (kMetaOff + kMetaBytes + 15) & ~15;
+    static constexpr int kSmem = kBarOff + (3 * kStages + 1) * 8 + 16;
     static_assert(kSmem <= 227 * 1024, "shared memory budget");
+    static_assert(kStage % 1024 == 0 && kATileBytes % 1024 == 0, "swizzled tiles need 1024-byte alignment");
+    static_assert(kStagingOff % 16 == 0 && kStagingBytes % 16 == 0 && kPendOff % 16 == 0, "16-byte alignment");
+    static_assert(kMetaOff % 16 == 0 && kBarOff % 16 == 0, "16-byte aligned regions");
 };
 
+// Warp roles (192 threads):
+//   warp 4 (loader): per chunk, lane 0 acquires the stage ("empty"), records
+//     the chunk in the stage's pending record, sets the "full" transaction
+//     count, and issues the dense A image (16 KB cp.async.bulk) or the sparse
+//     entries (cp.async.bulk into staging, completing on "staged"); then the
+//     32 lanes issue the B gather: 16 row groups x NT/64 boxes of
+//     tile::gather4 (4 rows x 128 bytes each, 128-byte swizzle), completing on
+//     "full". Nothing in the loader waits for data, so it runs up to kStages
+//     chunks ahead of the tensor core.
+//   warps 0-3 (scatter): per chunk, wait "staged"; for a sparse chunk zero the
+//     A tile, scatter the staged entries into the 128-byte swizzled K-major
+//     layout and fence.proxy.async; arrive on "full".
+//   warp 5, lane 0 (MMA): wait "full", 4 x tcgen05.mma, commit "empty"; after
+//     the last chunk commit "accumulator ready".
+//   warps 0-3 (epilogue): warp w reads TMEM lanes 32w .. 32w + 31 (rows).
 template <int NT, typename OutT>
 __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_constant__ TcBatch batch)
 {
     using Cfg = TcCfg<NT>;
     constexpr int S = Cfg::kStages;
-    constexpr int kPiecesPerRow = NT / 8; // 16-byte pieces of one B row slice
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    int *meta_cols = reinterpret_cast<int *>(smem + Cfg::kMetaOff);
-    int *meta_eptr = meta_cols + kMetaChunks * kChunkCols; // kMetaChunks + 1
-    int *meta_img = meta_eptr + kMetaChunks + 1;           // kMetaChunks
+    constexpr int kBoxes = NT / 64;      // 64-column boxes per B row slice
+    constexpr int kGathers = 16 * kBoxes; // gather4 instructions per chunk
+    extern __shared__ __align__(1024) uint8_t smem[];
+    int4 *pend = reinterpret_cast<int4 *>(smem + Cfg::kPendOff);
+    int *meta_cols = reinterpret_cast<int *>(smem + Cfg::kMetaOff); // kMetaChunks x 64 columns
+    int *meta_img = meta_cols + kMetaChunks * kChunkCols;           // kMetaChunks image indices
+    int *meta_eptr = meta_img + kMetaChunks;                        // kMetaChunks + 1 entry offsets
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + Cfg::kBarOff);
     uint64_t *empty = full + S;
-    uint64_t *accum = empty + S;
-    volatile int *flag = reinterpret_cast<volatile int *>(accum + 1);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accum + 1) + 1;
+    uint64_t *staged = empty + S;
+    uint64_t *accum = staged + S;
+    volatile int *flag = reinterpret_cast<volatile int *>(accum + 1); // 2 slots, alternating by chunk
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accum + 1) + 2;
 
     // ---- work item -> (job, window, N slice)
     const int item = blockIdx.x;
@@ -244,19 +297,25 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     const int local = item - batch.item_start[j];
     const int t = local / a.ntiles;
     const int n0 = (local % a.ntiles) * NT;
-    const int w = a.tc_windows[t];
-    const int c0 = a.tile_first[t], nch = a.tile_first[t + 1] - c0;
+    const int4 wi = a.win_info[t];
+    const int w = wi.x, c0 = wi.y, nch = wi.z;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (smem_u32(smem) & 1023u) { // the swizzled tiles and TMA destinations need a 1024-byte aligned base
+        if (threadIdx.x == 0)
+            atomicOr(a.status, kStatusLayout);
+        return;
+    }
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; s++) {
-            mbar_init(&full[s], kProducerThreads);
+            mbar_init(&full[s], kScatterThreads);
             mbar_init(&empty[s], 1);
+            mbar_init(&staged[s], 1);
         }
         mbar_init(accum, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 4) {
+    if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(NT)
                      : "memory");
@@ -268,88 +327,92 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
 
+    // The epilogue row of this thread (warps 0-3), fetched now so its latency
+    // hides behind the main loop; -1 = no store.
+    int out_row = -1;
     if (warp < 4) {
-        // ---------------- producers ----------------
-        // Chunk i is issued in iteration i and finished (copies waited for,
-        // sparse entries scattered, "full" signalled) in iteration i + S - 1,
-        // so up to S chunks of copies are in flight per CTA.
-        const int tid = threadIdx.x;
-        uint8_t *staging = smem + Cfg::kStagingOff;
-        int4 *pend = reinterpret_cast<int4 *>(smem + Cfg::kPendOff); // per stage: img, e0, e0a, e1
+        const int i = w * kWindowRows + warp * 32 + lane;
+        if (i < a.M && !((a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) && a.p_row_ptr[i + 1] == a.p_row_ptr[i]))
+            out_row = a.perm[i];
+    }
 
-        auto finish = [&](int idx, bool drain) {
-            if (drain) cp_async_wait<0>(); else cp_async_wait<S - 1>();
-            named_bar_sync(1, kProducerThreads); // every producer's copies of this chunk have landed
-            const int s = idx % S;
+    if (warp == kLoaderWarp) {
+        // ---------------- loader ----------------
+        for (int i = 0; i < nch; i++) {
+            const int s = i % S, mi = i % kMetaChunks;
+            if (mi == 0) { // metadata of the next up to kMetaChunks chunks
+                const int cnt = min(kMetaChunks, nch - i);
+                const int *src = a.win_cols + (size_t)(c0 + i) * kChunkCols;
+                for (int k = lane; k < cnt * kChunkCols; k += 32) meta_cols[k] = __ldg(src + k);
+                if (lane < cnt) meta_img[lane] = __ldg(a.img_idx + c0 + i + lane);
+                if (lane <= cnt) meta_eptr[lane] = __ldg(a.tile_ptr + c0 + i + lane);
+                __syncwarp();
+            }
+            uint32_t got = 1;
+            if (lane == 0 && i >= S)
+                got = mbar_wait(&empty[s], ((i / S) - 1) & 1) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) { ok = false; break; }
+            const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
+            const int img = meta_img[mi];
+            if (lane == 0) {
+                const int e0 = meta_eptr[mi], e1 = meta_eptr[mi + 1], e0a = e0 & ~3;
+                pend[s] = make_int4(img, e0, e0a, e1);
+                mbar_expect_tx(&full[s], Cfg::kBTileBytes + (img >= 0 ? kATileBytes : 0));
+                if (img >= 0) {
+                    bulk_copy_g2s(a_s, a.images + (size_t)img * (kATileBytes / 2), kATileBytes, &full[s]);
+                    mbar_arrive(&staged[s]);
+                } else if (e1 > e0) {
+                    const uint32_t bytes = (uint32_t)(((e1 - e0a) * 4 + 15) & ~15);
+                    mbar_arrive_expect_tx(&staged[s], bytes);
+                    bulk_copy_g2s(smem_u32(smem + Cfg::kStagingOff + s * kStagingBytes), a.entries + e0a, bytes,
+                                  &staged[s]);
+                } else {
+                    mbar_arrive(&staged[s]);
+                }
+            }
+            __syncwarp(); // the transaction count is set before any gather is issued
+            const int *cols = meta_cols + mi * kChunkCols;
+            if (cols[0] >= 0 && cols[kChunkCols - 1] == cols[0] + kChunkCols - 1) {
+                // 64 contiguous B rows (direct chunks): one 8 KB tiled box per 64 columns
+                if (lane < kBoxes)
+                    tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * 64, cols[0], &full[s]);
+            } else {
+                for (int q = lane; q < kGathers; q += 32) {
+                    const int g = q & 15, box = q >> 4;
+                    tma_gather4(b_s + box * (kChunkCols * 128) + g * 512, &a.tmap_b, n0 + box * 64, cols[4 * g],
+                                cols[4 * g + 1], cols[4 * g + 2], cols[4 * g + 3], &full[s]);
+                }
+            }
+            __syncwarp(); // the metadata cache is reloaded only after every lane used it
+        }
+    } else if (warp < 4) {
+        // ---------------- scatter ----------------
+        const int sid = threadIdx.x;
+        for (int i = 0; i < nch; i++) {
+            const int s = i % S;
+            if (sid == 0)
+                flag[i & 1] = mbar_wait(&staged[s], (i / S) & 1) ? 1 : 0;
+            named_bar_sync(1, kScatterThreads); // also orders the staged data for every scatter thread
+            if (flag[i & 1] == 0) { ok = false; break; } // uniform across the scatter warps
             const int4 pd = pend[s];
             if (pd.x < 0) {
                 uint8_t *At = smem + s * Cfg::kStage;
-                const uint32_t *st = reinterpret_cast<const uint32_t *>(staging + s * kStagingBytes);
-                for (int e = pd.y + tid; e < pd.w; e += kProducerThreads) {
+#pragma unroll
+                for (int k = 0; k < kATileBytes / (16 * kScatterThreads); k++)
+                    reinterpret_cast<uint4 *>(At)[sid + k * kScatterThreads] = make_uint4(0, 0, 0, 0);
+                named_bar_sync(1, kScatterThreads);
+                const uint32_t *st = reinterpret_cast<const uint32_t *>(smem + Cfg::kStagingOff + s * kStagingBytes);
+                for (int e = pd.y + sid; e < pd.w; e += kScatterThreads) {
                     const uint32_t v = st[e - pd.z];
                     *reinterpret_cast<uint16_t *>(At + swz128_offset(v >> 22, (v >> 16) & 63u)) =
                         (uint16_t)(v & 0xffffu);
                 }
+                fence_proxy_async();
             }
-            fence_proxy_async();
             mbar_arrive(&full[s]);
-        };
-
-        for (int i = 0; i < nch; i++) {
-            const int s = i % S, mi = i % kMetaChunks;
-            if (mi == 0) { // (re)load the metadata of up to kMetaChunks chunks
-                named_bar_sync(1, kProducerThreads);
-                const int cnt = min(kMetaChunks, nch - i);
-                const int *src = a.win_cols + (size_t)(c0 + i) * kChunkCols;
-                for (int k = tid; k < cnt * kChunkCols; k += kProducerThreads) meta_cols[k] = __ldg(src + k);
-                for (int k = tid; k <= cnt; k += kProducerThreads) meta_eptr[k] = __ldg(a.tile_ptr + c0 + i + k);
-                for (int k = tid; k < cnt; k += kProducerThreads) meta_img[k] = __ldg(a.img_idx + c0 + i + k);
-                named_bar_sync(1, kProducerThreads);
-            }
-            if (tid == 0)
-                *flag = (i < S) ? 1 : (mbar_wait(&empty[s], ((i / S) - 1) & 1) ? 1 : 0);
-            named_bar_sync(1, kProducerThreads);
-            if (*flag == 0) { ok = false; break; } // uniform across the producers
-            uint8_t *At = smem + s * Cfg::kStage;
-            const uint32_t a_s = smem_u32(At), b_s = a_s + kATileBytes;
-            const int img = meta_img[mi];
-            const int e0 = meta_eptr[mi], e1 = meta_eptr[mi + 1], e0a = e0 & ~3;
-            if (tid == 0)
-                pend[s] = make_int4(img, e0, e0a, e1); // read after the barrier in finish(i)
-            if (img >= 0) {
-                if (tid == 0) {
-                    mbar_expect_tx(&full[s], kATileBytes);
-                    bulk_copy_g2s(a_s, a.images + (size_t)img * (kATileBytes / 2), kATileBytes, &full[s]);
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < kATileBytes / (16 * kProducerThreads); k++)
-                    reinterpret_cast<uint4 *>(At)[tid + k * kProducerThreads] = make_uint4(0, 0, 0, 0);
-                const uint32_t st_s = smem_u32(staging + s * kStagingBytes);
-                const int pieces = (e1 - e0a + 3) >> 2;
-                for (int k = tid; k < pieces; k += kProducerThreads)
-                    cp_async16(st_s + k * 16, a.entries + e0a + 4 * k, 16u);
-            }
-            const int *cols = meta_cols + mi * kChunkCols;
-#pragma unroll 4
-            for (int piece = tid; piece < kChunkCols * kPiecesPerRow; piece += kProducerThreads) {
-                const int k = piece / kPiecesPerRow, qq = piece % kPiecesPerRow;
-                const int col = cols[k];
-                const int n = n0 + qq * 8;
-                const bool valid = (col >= 0) && (n < a.N);
-                const __half *src = valid ? (a.B + (size_t)col * a.ldb + n) : a.B;
-                const uint32_t dst = b_s + (qq >> 3) * (kChunkCols * 128) + k * 128 + ((((qq & 7) ^ (k & 7))) << 4);
-                cp_async16(dst, src, valid ? 16u : 0u);
-            }
-            cp_async_commit();
-            if (i >= S - 1)
-                finish(i - (S - 1), false);
         }
-        if (ok)
-            for (int idx = max(0, nch - (S - 1)); idx < nch; idx++)
-                finish(idx, true);
-        cp_async_wait<0>(); // no copy outlives the CTA, also on the abort path
-    } else if (lane == 0) {
+    } else if (warp == kMmaWarp && lane == 0) {
         // ---------------- MMA issuer ----------------
         constexpr uint32_t idesc = idesc_f16(NT);
         for (int i = 0; i < nch; i++) {
@@ -377,15 +440,8 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         got = __shfl_sync(0xffffffffu, got, 0);
         tc_fence_after();
         if (got) {
-            const int i = w * kWindowRows + warp * 32 + lane;
-            const bool valid = i < a.M;
-            bool write = valid;
-            OutT *Crow = nullptr;
-            if (valid) {
-                if ((a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) && a.p_row_ptr[i + 1] == a.p_row_ptr[i])
-                    write = false;
-                Crow = reinterpret_cast<OutT *>(a.C) + (size_t)a.perm[i] * a.ldc;
-            }
+            const bool write = out_row >= 0;
+            OutT *Crow = write ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
             for (int cb = 0; cb < NT / 16; cb++) {
                 const int n = n0 + cb * 16;
                 if (n >= a.N)
@@ -407,18 +463,52 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         atomicOr(a.status, kStatusTimeout);
     tc_fence_before();
     __syncthreads();
-    if (warp == 4) {
+    if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NT) : "memory");
     }
 }
 
-TcJob make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// B (K x N, row-major, leading dimension ldb) as a TMA source: dims {N, K},
+// row stride ldb * 2 bytes, box {64, rows}, 128-byte swizzle, zero fill.
+int encode_b_map(const SpmmJob &sj, int K, int rows, CUtensorMap *map)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc)
+        return set_error(TCA_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[2] = {(cuuint64_t)sj.N, (cuuint64_t)(K > 0 ? K : 1)};
+    const cuuint64_t strides[1] = {(cuuint64_t)sj.ldb * 2};
+    const cuuint32_t box[2] = {64, (cuuint32_t)rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<__half *>(sj.B), dims, strides, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return set_error(TCA_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) for B (N=%d, ldb=%d)", (int)r, sj.N, sj.ldb);
+    return TCA_OK;
+}
+
+int make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT, TcJob *out)
 {
     const tca_plan *p = sj.p;
-    TcJob j;
-    j.tc_windows = p->tc_windows;
-    j.tile_first = p->tile_first;
+    TcJob &j = *out;
+    TCA_TRY(encode_b_map(sj, p->K, 1, &j.tmap_b));
+    TCA_TRY(encode_b_map(sj, p->K, kChunkCols, &j.tmap_tile));
+    j.win_info = p->tc_win_info;
     j.tile_ptr = p->tile_ptr;
     j.win_cols = p->win_cols;
     j.img_idx = p->img_idx;
@@ -437,7 +527,7 @@ TcJob make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int N
     j.alpha = alpha;
     j.beta = beta;
     j.flags = flags;
-    return j;
+    return TCA_OK;
 }
 
 template <int NT, typename OutT>
@@ -491,9 +581,8 @@ int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
             const SpmmJob &sj = jobs[i];
             if (!sj.tc || sj.n_tile != NT || sj.p->n_tc == 0 || sj.N <= 0)
                 continue;
-            const TcJob j = make_job(sj, alpha, beta, flags, NT);
-            b.job[b.n_jobs] = j;
-            b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + sj.p->n_tc * j.ntiles;
+            TCA_TRY(make_job(sj, alpha, beta, flags, NT, &b.job[b.n_jobs]));
+            b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + sj.p->n_tc * b.job[b.n_jobs].ntiles;
             b.n_jobs++;
             if (b.n_jobs == kMaxJobs) {
                 TCA_TRY(launch_group_typed(b, NT, c_dtype, s));
