@@ -174,6 +174,23 @@ typedef struct tca_batch_item {
  * so the call can be captured in a CUDA graph. */
 TCA_API int tca_spmm_batched(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha,
                              float beta, unsigned flags, tca_stream_t stream, void *const *events);
+/* ------------------------------------------------------------------ */
+/* Adjoints of Y = A B (the reference has no backward pass; these follow
+ * from its forward, src/our_spmm.cu:290-346, Y[r,:] = sum_j a_j B[c_j,:]).  */
+/* ------------------------------------------------------------------ */
+/* dA on A's pattern (SDDMM): out[j] = alpha * sum_n dY[r_j, n] * B[c_j, n]
+ * for every nonzero j in the caller's CSR order; dY is M x N (ldy), B is
+ * K x N (ldb), out is nnz values of out_dtype (F16 or F32). */
+TCA_API int tca_sddmm(tca_plan_t plan, const void *d_dY_f16, int ldy, const void *d_B_f16, int ldb, int N,
+                      void *d_out, int out_dtype, float alpha, tca_stream_t stream);
+/* dB = alpha * A^T dY + beta * dB (dY M x N, dB K x N of dB_dtype). Runs the
+ * forward kernels on a plan of A^T, which the first call builds on the GPU
+ * (allocating; do that call, or tca_plan_build_transpose, outside stream
+ * capture). tca_plan_update_values keeps A^T's values in step. */
+TCA_API int tca_spmm_t(tca_plan_t plan, const void *d_dY_f16, int ldy, int N, void *d_dB, int lddb,
+                       int dB_dtype, float alpha, float beta, tca_stream_t stream);
+TCA_API int tca_plan_build_transpose(tca_plan_t plan, tca_stream_t stream);
+
 /* How many tensor-core and CUDA-core kernel launches one tca_spmm with this
  * N makes (0 or 1 each). */
 TCA_API int tca_plan_launch_counts(tca_plan_t plan, int N, int *n_tc_launches, int *n_cc_launches);

@@ -300,6 +300,7 @@ int dev_alloc(T **ptr, size_t count, size_t *bytes)
 void free_plan(tca_plan *p)
 {
     if (!p) return;
+    transpose_free(p);
     void *arrs[] = {p->perm, p->p_row_ptr, p->p_col, p->p_val, p->src, p->tc_windows, p->cc_windows,
                     p->all_windows, p->tile_first, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src,
                     p->img_idx, p->images, p->img_chunk, p->cc_items, p->all_items, p->tc_win_info,
@@ -598,7 +599,7 @@ int tca_plan_update_values(tca_plan_t p, const void *d_vals_f16, tca_stream_t st
     if (p->n_images > 0)
         k_render_images<<<p->n_images, 256, 0, s>>>(p->img_chunk, p->tile_ptr, p->tile_entries, p->images);
     TCA_CUDA_TRY(cudaGetLastError());
-    return TCA_OK;
+    return transpose_update_values(p, (const __half *)d_vals_f16, s);
 }
 
 int tca_plan_info(tca_plan_t p, tca_plan_info_t *info)

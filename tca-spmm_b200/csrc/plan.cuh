@@ -59,6 +59,12 @@ struct tca_plan {
     int n_cc_items = 0, n_all_items = 0;
     int *d_status = nullptr; // device error word written by bounded waits
     size_t bytes = 0;
+    // A^T as a plan of its own (built on first use by tca_spmm_t or by
+    // tca_plan_build_transpose), with t_src mapping each of its entries to the
+    // caller's nonzero index and t_vals the values in that order.
+    struct tca_plan *tplan = nullptr;
+    int *t_src = nullptr;
+    __half *t_vals = nullptr;
 };
 
 namespace tca {
@@ -105,6 +111,10 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
 
 // The N-slice width a single forward of this plan uses.
 int pick_tc_tile(int n_tc, int N, bool batched);
+
+// The plan of A^T (adjoint.cu): propagate new caller-order values; release.
+int transpose_update_values(tca_plan *p, const __half *vals, cudaStream_t s);
+void transpose_free(tca_plan *p);
 
 // Whether B/C of a forward allow the vectorised and tensor-core kernels.
 bool dense_operands_vec_ok(const void *B, int ldb, int N, const void *C, int ldc, int c_dtype);

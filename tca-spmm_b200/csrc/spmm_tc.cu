@@ -32,6 +32,7 @@
 // completion without hanging. No load uses cluster multicast.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <algorithm>
 #include <mutex>
 #include "tca_internal.cuh"
 #include "plan.cuh"
@@ -39,13 +40,16 @@
 namespace tca {
 namespace {
 
-constexpr int kScatterThreads = 128; // warps 0-3: scatter, then epilogue
+constexpr int kScatterThreads = 128; // warps 0-3: sparse-entry scatter
 constexpr int kLoaderWarp = 4;       // TMA issue
 constexpr int kMmaWarp = 5;          // TMEM allocation, tcgen05.mma issue
-constexpr int kThreads = 192;
+constexpr int kEpiThreads = 128;     // warps 6-9: epilogue
+constexpr int kThreads = 320;
+constexpr int kMetaRing = 8;          // chunk-metadata prefetch ring (prefetch distance kMetaRing - 1)
+constexpr int kMetaSlotInts = 68;     // 64 columns, image index, first and end entry, pad
+constexpr int kMaxCtaItems = 32;      // work items per persistent CTA
 constexpr int kATileBytes = kWindowRows * kChunkCols * 2;     // 16 KB
 constexpr int kStagingBytes = ((kImageMinNnz + 3) * 4 + 15) & ~15; // entries of a sparse chunk, 16-byte rounded
-constexpr int kMetaChunks = 8;                                // chunk metadata cached in shared memory
 constexpr int kMaxJobs = 32;                                  // jobs per launch (kernel parameter space)
 
 struct TcJob {
@@ -236,74 +240,97 @@ __device__ __forceinline__ void store8_out(float *p, const float *v, float alpha
 }
 
 // Shared memory (1024-byte aligned base): kStages x (A tile | B tile),
-// kStages entry staging buffers, per-stage pending-chunk records, the loader's
-// chunk metadata cache, mbarriers (full, empty, staged per stage; accumulator
-// ready), two broadcast flags and the TMEM address slot.
+// kStages entry staging buffers, per-stage chunk records, the chunk-metadata
+// ring, the CTA's item table, mbarriers and two broadcast flags + TMEM slot.
 template <int NT> struct TcCfg {
-    static constexpr int kStages = NT == 256 ? 4 : NT == 128 ? 5 : 7;
+    static constexpr int kStages = NT == 256 ? 4 : NT == 128 ? 5 : 6;
     static constexpr int kBTileBytes = kChunkCols * NT * 2;
     static constexpr int kStage = kATileBytes + kBTileBytes;
     static constexpr int kStagingOff = kStages * kStage;
-    static constexpr int kPendOff = kStagingOff + kStages * kStagingBytes;
-    static constexpr int kMetaOff = kPendOff + kStages * 16;
-    static constexpr int kMetaBytes = (kMetaChunks * kChunkCols + 2 * kMetaChunks + 1) * 4;
-    static constexpr int kBarOff = (kMetaOff + kMetaBytes + 15) & ~15;
-    static constexpr int kSmem = kBarOff + (3 * kStages + 1) * 8 + 16;
+    static constexpr int kPendOff = kStagingOff + kStages * kStagingBytes; // int4 [kStages]: img, e0, e0a, e1
+    static constexpr int kPend2Off = kPendOff + kStages * 16;              // int4 [kStages]: flags, buffer, item
+    static constexpr int kMetaOff = kPend2Off + kStages * 16;              // int [kMetaRing][kMetaSlotInts]
+    static constexpr int kItemOff = kMetaOff + kMetaRing * kMetaSlotInts * 4; // int4 [kMaxCtaItems]
+    static constexpr int kBarOff = kItemOff + kMaxCtaItems * 16;
+    // full, empty, staged [kStages]; accum_full, accum_empty [2]
+    static constexpr int kSmem = kBarOff + (3 * kStages + 4) * 8 + 16;
     static_assert(kSmem <= 227 * 1024, "shared memory budget");
     static_assert(kStage % 1024 == 0 && kATileBytes % 1024 == 0, "swizzled tiles need 1024-byte alignment");
     static_assert(kStagingOff % 16 == 0 && kStagingBytes % 16 == 0 && kPendOff % 16 == 0, "16-byte alignment");
-    static_assert(kMetaOff % 16 == 0 && kBarOff % 16 == 0, "16-byte aligned regions");
+    static_assert(kMetaOff % 16 == 0 && kItemOff % 16 == 0 && kBarOff % 16 == 0, "16-byte aligned regions");
 };
 
-// Warp roles (192 threads):
-//   warp 4 (loader): per chunk, lane 0 acquires the stage ("empty"), records
-//     the chunk in the stage's pending record, sets the "full" transaction
-//     count, and issues the dense A image (16 KB cp.async.bulk) or the sparse
-//     entries (cp.async.bulk into staging, completing on "staged"); then the
-//     32 lanes issue the B gather: 16 row groups x NT/64 boxes of
-//     tile::gather4 (4 rows x 128 bytes each, 128-byte swizzle), completing on
-//     "full". Nothing in the loader waits for data, so it runs up to kStages
-//     chunks ahead of the tensor core.
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Work item (job, tensor-core window, N slice) -> table entry {window,
+// first chunk, chunk count, job << 16 | N-slice index}.
+__device__ __forceinline__ int4 decode_item(const TcBatch &batch, int item)
+{
+    int j = 0;
+    while (j + 1 < batch.n_jobs && batch.item_start[j + 1] <= item) j++;
+    const TcJob &a = batch.job[j];
+    const int local = item - batch.item_start[j];
+    const int4 wi = a.win_info[local / a.ntiles];
+    return make_int4(wi.x, wi.y, wi.z, (j << 16) | (local % a.ntiles));
+}
+
+// Persistent CTAs, one per SM: CTA b processes work items b, b + gridDim.x,
+// ... (at most kMaxCtaItems), as one continuous stream of chunks through the
+// stage ring. Warp roles (320 threads):
+//   warp 4 (loader): per chunk, acquire the stage ("empty"), write the
+//     chunk's records (entries range and image for the scatter warps; first /
+//     last chunk of its item and accumulator buffer for the MMA lane), set the
+//     "full" transaction count and issue the dense A image (16 KB
+//     cp.async.bulk) or the sparse entries (cp.async.bulk into staging,
+//     completing on "staged"), then the B rows: tiled TMA boxes of 64
+//     contiguous rows for direct chunks, tile::gather4 for condensed ones.
+//     Chunk metadata is prefetched kMetaRing - 1 chunks ahead with cp.async.
+//     After the last chunk it passes an end record through the ring.
 //   warps 0-3 (scatter): per chunk, wait "staged"; for a sparse chunk zero the
-//     A tile, scatter the staged entries into the 128-byte swizzled K-major
-//     layout and fence.proxy.async; arrive on "full".
-//   warp 5, lane 0 (MMA): wait "full", 4 x tcgen05.mma, commit "empty"; after
-//     the last chunk commit "accumulator ready".
-//   warps 0-3 (epilogue): warp w reads TMEM lanes 32w .. 32w + 31 (rows).
+//     A tile, scatter the staged entries, fence.proxy.async; arrive "full".
+//   warp 5, lane 0 (MMA): per chunk wait "full"; on an item's first chunk
+//     wait until its TMEM accumulator buffer (item parity) is drained
+//     ("accum_empty"); 4 x tcgen05.mma; commit "empty"; on the item's last
+//     chunk commit "accum_full".
+//   warps 6-9 (epilogue): per item wait "accum_full", tcgen05.ld the rows
+//     (warp w reads TMEM lanes 32 (w % 4) ..), alpha/beta, store to C[perm],
+//     arrive "accum_empty" -- overlapping the next item's main loop.
 template <int NT, typename OutT>
 __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_constant__ TcBatch batch)
 {
     using Cfg = TcCfg<NT>;
     constexpr int S = Cfg::kStages;
-    constexpr int kBoxes = NT / 64;      // 64-column boxes per B row slice
-    constexpr int kGathers = 16 * kBoxes; // gather4 instructions per chunk
+    constexpr int kBoxes = NT / 64;       // 64-column boxes per B row slice
+    constexpr int kGathers = 16 * kBoxes; // gather4 instructions per condensed chunk
+    constexpr int P = kMetaRing - 1;      // metadata prefetch distance
     extern __shared__ __align__(1024) uint8_t smem[];
     int4 *pend = reinterpret_cast<int4 *>(smem + Cfg::kPendOff);
-    int *meta_cols = reinterpret_cast<int *>(smem + Cfg::kMetaOff); // kMetaChunks x 64 columns
-    int *meta_img = meta_cols + kMetaChunks * kChunkCols;           // kMetaChunks image indices
-    int *meta_eptr = meta_img + kMetaChunks;                        // kMetaChunks + 1 entry offsets
+    int4 *pend2 = reinterpret_cast<int4 *>(smem + Cfg::kPend2Off);
+    int *meta = reinterpret_cast<int *>(smem + Cfg::kMetaOff);
+    int4 *items = reinterpret_cast<int4 *>(smem + Cfg::kItemOff);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + Cfg::kBarOff);
     uint64_t *empty = full + S;
     uint64_t *staged = empty + S;
-    uint64_t *accum = staged + S;
-    volatile int *flag = reinterpret_cast<volatile int *>(accum + 1); // 2 slots, alternating by chunk
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accum + 1) + 2;
-
-    // ---- work item -> (job, window, N slice)
-    const int item = blockIdx.x;
-    int j = 0;
-    while (j + 1 < batch.n_jobs && batch.item_start[j + 1] <= item) j++;
-    const TcJob &a = batch.job[j];
-    const int local = item - batch.item_start[j];
-    const int t = local / a.ntiles;
-    const int n0 = (local % a.ntiles) * NT;
-    const int4 wi = a.win_info[t];
-    const int w = wi.x, c0 = wi.y, nch = wi.z;
+    uint64_t *acc_full = staged + S;  // [2]
+    uint64_t *acc_empty = acc_full + 2; // [2]
+    volatile int *flag = reinterpret_cast<volatile int *>(acc_empty + 2); // 2 slots, alternating by chunk
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + 2) + 2;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = batch.item_start[batch.n_jobs];
+    const int n_items = blockIdx.x < total ? min(kMaxCtaItems, (total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1) : 0;
     if (smem_u32(smem) & 1023u) { // the swizzled tiles and TMA destinations need a 1024-byte aligned base
-        if (threadIdx.x == 0)
-            atomicOr(a.status, kStatusLayout);
+        if (threadIdx.x == 0 && n_items > 0)
+            atomicOr(batch.job[0].status, kStatusLayout);
         return;
     }
     if (threadIdx.x == 0) {
@@ -312,12 +339,17 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             mbar_init(&empty[s], 1);
             mbar_init(&staged[s], 1);
         }
-        mbar_init(accum, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], kEpiThreads);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if ((int)threadIdx.x < n_items)
+        items[threadIdx.x] = decode_item(batch, blockIdx.x + threadIdx.x * gridDim.x);
     if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(NT)
+                     "r"(2 * NT)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -327,76 +359,104 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
 
-    // The epilogue row of this thread (warps 0-3), fetched now so its latency
-    // hides behind the main loop; -1 = no store.
-    int out_row = -1;
-    if (warp < 4) {
-        const int i = w * kWindowRows + warp * 32 + lane;
-        if (i < a.M && !((a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) && a.p_row_ptr[i + 1] == a.p_row_ptr[i]))
-            out_row = a.perm[i];
-    }
-
     if (warp == kLoaderWarp) {
         // ---------------- loader ----------------
-        for (int i = 0; i < nch; i++) {
-            const int s = i % S, mi = i % kMetaChunks;
-            if (mi == 0) { // metadata of the next up to kMetaChunks chunks
-                const int cnt = min(kMetaChunks, nch - i);
-                const int *src = a.win_cols + (size_t)(c0 + i) * kChunkCols;
-                for (int k = lane; k < cnt * kChunkCols; k += 32) meta_cols[k] = __ldg(src + k);
-                if (lane < cnt) meta_img[lane] = __ldg(a.img_idx + c0 + i + lane);
-                if (lane <= cnt) meta_eptr[lane] = __ldg(a.tile_ptr + c0 + i + lane);
-                __syncwarp();
+        // prefetch cursor: (item k, chunk i) of the next chunk whose metadata to fetch
+        int pk = 0, pi = 0;
+        auto prefetch = [&](int slot) {
+            if (pk < n_items) {
+                const int4 it = items[pk];
+                const TcJob &a = batch.job[it.w >> 16];
+                const int c = it.y + pi;
+                const uint32_t dst = smem_u32(meta + slot * kMetaSlotInts);
+                if (lane < 16)
+                    cp_async16(dst + lane * 16, a.win_cols + (size_t)c * kChunkCols + lane * 4);
+                else if (lane == 16)
+                    cp_async4(dst + 64 * 4, a.img_idx + c);
+                else if (lane == 17)
+                    cp_async4(dst + 65 * 4, a.tile_ptr + c);
+                else if (lane == 18)
+                    cp_async4(dst + 66 * 4, a.tile_ptr + c + 1);
+                if (++pi == it.z) { pi = 0; pk++; }
             }
-            uint32_t got = 1;
-            if (lane == 0 && i >= S)
-                got = mbar_wait(&empty[s], ((i / S) - 1) & 1) ? 1u : 0u;
-            got = __shfl_sync(0xffffffffu, got, 0);
-            if (!got) { ok = false; break; }
-            const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
-            const int img = meta_img[mi];
-            if (lane == 0) {
-                const int e0 = meta_eptr[mi], e1 = meta_eptr[mi + 1], e0a = e0 & ~3;
-                pend[s] = make_int4(img, e0, e0a, e1);
-                mbar_expect_tx(&full[s], Cfg::kBTileBytes + (img >= 0 ? kATileBytes : 0));
-                if (img >= 0) {
-                    bulk_copy_g2s(a_s, a.images + (size_t)img * (kATileBytes / 2), kATileBytes, &full[s]);
-                    mbar_arrive(&staged[s]);
-                } else if (e1 > e0) {
-                    const uint32_t bytes = (uint32_t)(((e1 - e0a) * 4 + 15) & ~15);
-                    mbar_arrive_expect_tx(&staged[s], bytes);
-                    bulk_copy_g2s(smem_u32(smem + Cfg::kStagingOff + s * kStagingBytes), a.entries + e0a, bytes,
-                                  &staged[s]);
+            cp_async_commit();
+        };
+        for (int q = 0; q < P; q++) prefetch(q);
+        int g = 0;
+        for (int k = 0; k < n_items && ok; k++) {
+            const int4 it = items[k];
+            const TcJob &a = batch.job[it.w >> 16];
+            const int n0 = (it.w & 0xffff) * NT;
+            for (int i = 0; i < it.z; i++, g++) {
+                const int s = g % S;
+                uint32_t got = 1;
+                if (lane == 0 && g >= S)
+                    got = mbar_wait(&empty[s], ((g / S) - 1) & 1) ? 1u : 0u;
+                got = __shfl_sync(0xffffffffu, got, 0);
+                if (!got) { ok = false; break; }
+                cp_async_wait<P - 1>(); // this chunk's metadata has landed (this lane's share)
+                __syncwarp();           // ... and every lane's
+                const int *m = meta + (g % kMetaRing) * kMetaSlotInts;
+                const int img = m[64];
+                const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
+                if (lane == 0) {
+                    const int e0 = m[65], e1 = m[66], e0a = e0 & ~3;
+                    pend[s] = make_int4(img, e0, e0a, e1);
+                    pend2[s] = make_int4((i == 0 ? 1 : 0) | (i == it.z - 1 ? 2 : 0), k & 1, k, 0);
+                    mbar_expect_tx(&full[s], Cfg::kBTileBytes + (img >= 0 ? kATileBytes : 0));
+                    if (img >= 0) {
+                        bulk_copy_g2s(a_s, a.images + (size_t)img * (kATileBytes / 2), kATileBytes, &full[s]);
+                        mbar_arrive(&staged[s]);
+                    } else if (e1 > e0) {
+                        const uint32_t bytes = (uint32_t)(((e1 - e0a) * 4 + 15) & ~15);
+                        mbar_arrive_expect_tx(&staged[s], bytes);
+                        bulk_copy_g2s(smem_u32(smem + Cfg::kStagingOff + s * kStagingBytes), a.entries + e0a, bytes,
+                                      &staged[s]);
+                    } else {
+                        mbar_arrive(&staged[s]);
+                    }
+                }
+                __syncwarp(); // the transaction count is set before any B load is issued
+                if (m[0] >= 0 && m[kChunkCols - 1] == m[0] + kChunkCols - 1) {
+                    // 64 contiguous B rows (direct chunks): one 8 KB tiled box per 64 columns
+                    if (lane < kBoxes)
+                        tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * 64, m[0], &full[s]);
                 } else {
-                    mbar_arrive(&staged[s]);
+                    for (int q = lane; q < kGathers; q += 32) {
+                        const int gg = q & 15, box = q >> 4;
+                        tma_gather4(b_s + box * (kChunkCols * 128) + gg * 512, &a.tmap_b, n0 + box * 64, m[4 * gg],
+                                    m[4 * gg + 1], m[4 * gg + 2], m[4 * gg + 3], &full[s]);
+                    }
                 }
+                __syncwarp(); // every lane has read slot g before it is refilled
+                prefetch((g + P) % kMetaRing);
             }
-            __syncwarp(); // the transaction count is set before any gather is issued
-            const int *cols = meta_cols + mi * kChunkCols;
-            if (cols[0] >= 0 && cols[kChunkCols - 1] == cols[0] + kChunkCols - 1) {
-                // 64 contiguous B rows (direct chunks): one 8 KB tiled box per 64 columns
-                if (lane < kBoxes)
-                    tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * 64, cols[0], &full[s]);
-            } else {
-                for (int q = lane; q < kGathers; q += 32) {
-                    const int g = q & 15, box = q >> 4;
-                    tma_gather4(b_s + box * (kChunkCols * 128) + g * 512, &a.tmap_b, n0 + box * 64, cols[4 * g],
-                                cols[4 * g + 1], cols[4 * g + 2], cols[4 * g + 3], &full[s]);
-                }
-            }
-            __syncwarp(); // the metadata cache is reloaded only after every lane used it
         }
+        // end record: scatter warps and the MMA lane stop at it
+        if (ok) {
+            const int s = g % S;
+            uint32_t got = 1;
+            if (lane == 0 && g >= S)
+                got = mbar_wait(&empty[s], ((g / S) - 1) & 1) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (got && lane == 0) {
+                pend[s] = make_int4(-2, 0, 0, 0);
+                mbar_arrive(&staged[s]);
+            }
+            if (!got) ok = false;
+        }
+        cp_async_wait<0>();
     } else if (warp < 4) {
         // ---------------- scatter ----------------
         const int sid = threadIdx.x;
-        for (int i = 0; i < nch; i++) {
-            const int s = i % S;
+        for (int g = 0;; g++) {
+            const int s = g % S;
             if (sid == 0)
-                flag[i & 1] = mbar_wait(&staged[s], (i / S) & 1) ? 1 : 0;
+                flag[g & 1] = mbar_wait(&staged[s], (g / S) & 1) ? 1 : 0;
             named_bar_sync(1, kScatterThreads); // also orders the staged data for every scatter thread
-            if (flag[i & 1] == 0) { ok = false; break; } // uniform across the scatter warps
+            if (flag[g & 1] == 0) { ok = false; break; } // uniform across the scatter warps
             const int4 pd = pend[s];
-            if (pd.x < 0) {
+            if (pd.x >= -1 && pd.x < 0) {
                 uint8_t *At = smem + s * Cfg::kStage;
 #pragma unroll
                 for (int k = 0; k < kATileBytes / (16 * kScatterThreads); k++)
@@ -411,61 +471,80 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                 fence_proxy_async();
             }
             mbar_arrive(&full[s]);
+            if (pd.x == -2)
+                break; // end record
         }
-    } else if (warp == kMmaWarp && lane == 0) {
+    } else if (warp == kMmaWarp) {
         // ---------------- MMA issuer ----------------
-        constexpr uint32_t idesc = idesc_f16(NT);
-        for (int i = 0; i < nch; i++) {
-            const int s = i % S;
-            if (!mbar_wait(&full[s], (i / S) & 1)) { ok = false; break; }
-            tc_fence_after();
-            const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_f16(NT);
+            for (int g = 0;; g++) {
+                const int s = g % S;
+                if (!mbar_wait(&full[s], (g / S) & 1)) { ok = false; break; }
+                const int4 pd = pend[s];
+                if (pd.x == -2)
+                    break; // end record
+                const int4 f = pend2[s];
+                const int b = f.y, k = f.z;
+                if ((f.x & 1) && k >= 2 && !mbar_wait(&acc_empty[b], ((k >> 1) - 1) & 1)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
+                const uint32_t d = tmem + (uint32_t)(b * NT);
 #pragma unroll
-            for (int k = 0; k < kChunkCols / 16; k++) {
-                const uint64_t ad = smem_desc(a_s + k * 32, 16, 1024);
-                const uint64_t bd = smem_desc(b_s + k * 2048, kChunkCols * 128, 1024);
-                umma_f16(tmem, ad, bd, idesc, (i | k) != 0);
+                for (int kk = 0; kk < kChunkCols / 16; kk++) {
+                    const uint64_t ad = smem_desc(a_s + kk * 32, 16, 1024);
+                    const uint64_t bd = smem_desc(b_s + kk * 2048, kChunkCols * 128, 1024);
+                    umma_f16(d, ad, bd, idesc, ((f.x & 1) && kk == 0) ? 0u : 1u);
+                }
+                umma_commit(&empty[s]);
+                if (f.x & 2)
+                    umma_commit(&acc_full[b]);
             }
-            umma_commit(&empty[s]);
         }
-        if (ok)
-            umma_commit(accum);
-    }
-
-    if (warp < 4) {
+        __syncwarp();
+    } else {
         // ---------------- epilogue ----------------
-        uint32_t got = 0;
-        if (lane == 0)
-            got = mbar_wait(accum, 0) ? 1u : 0u;
-        got = __shfl_sync(0xffffffffu, got, 0);
-        tc_fence_after();
-        if (got) {
-            const bool write = out_row >= 0;
-            OutT *Crow = write ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
+        const int quarter = warp & 3;
+        for (int k = 0; k < n_items; k++) {
+            const int4 it = items[k];
+            const TcJob &a = batch.job[it.w >> 16];
+            const int n0 = (it.w & 0xffff) * NT;
+            const int i = it.x * kWindowRows + quarter * 32 + lane;
+            int out_row = -1;
+            if (i < a.M && !((a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) && a.p_row_ptr[i + 1] == a.p_row_ptr[i]))
+                out_row = a.perm[i];
+            const int b = k & 1;
+            uint32_t got = 0;
+            if (lane == 0)
+                got = mbar_wait(&acc_full[b], (k >> 1) & 1) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) { ok = false; break; }
+            tc_fence_after();
+            OutT *Crow = out_row >= 0 ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
             for (int cb = 0; cb < NT / 16; cb++) {
                 const int n = n0 + cb * 16;
                 if (n >= a.N)
                     break; // uniform across the warp
                 uint32_t r[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 16), r);
-                if (write) {
+                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * NT + cb * 16), r);
+                if (Crow) {
                     store8_out(Crow + n, reinterpret_cast<const float *>(r), a.alpha, a.beta);
                     if (n + 8 < a.N)
                         store8_out(Crow + n + 8, reinterpret_cast<const float *>(r) + 8, a.alpha, a.beta);
                 }
             }
-        } else {
-            ok = false;
+            tc_fence_before();
+            mbar_arrive(&acc_empty[b]);
         }
     }
 
-    if (!ok)
-        atomicOr(a.status, kStatusTimeout);
+    if (!ok && n_items > 0)
+        atomicOr(batch.job[items[0].w >> 16].status, kStatusTimeout);
     tc_fence_before();
     __syncthreads();
     if (warp == kMmaWarp) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NT) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * NT) : "memory");
     }
 }
 
@@ -535,7 +614,9 @@ int launch_group(const TcBatch &b, cudaStream_t s)
 {
     const int smem = TcCfg<NT>::kSmem;
     TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    spmm_tc_kernel<NT, OutT><<<b.item_start[b.n_jobs], kThreads, smem, s>>>(b);
+    const int total = b.item_start[b.n_jobs];
+    const int grid = std::min(total, std::max(kSMs, (total + kMaxCtaItems - 1) / kMaxCtaItems));
+    spmm_tc_kernel<NT, OutT><<<grid, kThreads, smem, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
 }

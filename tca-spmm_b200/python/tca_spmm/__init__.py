@@ -86,6 +86,9 @@ _SIGS = {
     "tca_spmm_events": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP, ctypes.POINTER(_VP)], _I),
     "tca_plan_launch_counts": ([_VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
     "tca_spmm_batched": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _VP, ctypes.POINTER(_VP)], _I),
+    "tca_sddmm": ([_VP, _P, _I, _P, _I, _I, _P, _I, _F, _VP], _I),
+    "tca_spmm_t": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _VP], _I),
+    "tca_plan_build_transpose": ([_VP, _VP], _I),
     "tca_spmm_host": ([_P, _P, _P, _I, _I, _I, _P, _I, _P, _I, _U, _I, ctypes.POINTER(ctypes.c_double)], _I),
 }
 
@@ -258,6 +261,37 @@ class Plan:
         _check(self._lib.tca_spmm_events(self._h, _ptr(B), B.stride(0), N, _ptr(out), out.stride(0),
                                          _out_code(out.dtype), alpha, beta, flags, _stream_handle(stream), arr))
         return out
+
+    def sddmm(self, dY, B, out=None, out_dtype=None, alpha=1.0, stream=None):
+        """dA on the plan's pattern: out[j] = alpha * dot(dY[row_j], B[col_j]) in
+        the caller's nonzero order (tca_sddmm)."""
+        torch = _torch()
+        if dY.dim() != 2 or dY.dtype != torch.float16 or dY.stride(1) != 1 or dY.shape[0] != self.M:
+            raise ValueError("dY must be an M x N float16 tensor with unit column stride")
+        if B.dim() != 2 or B.dtype != torch.float16 or B.stride(1) != 1 or B.shape[1] != dY.shape[1]:
+            raise ValueError("B must be a K x N float16 tensor with unit column stride")
+        out_dtype = out_dtype or (out.dtype if out is not None else torch.float32)
+        if out is None:
+            out = torch.empty(self.nnz, dtype=out_dtype, device=dY.device)
+        _check(self._lib.tca_sddmm(self._h, _ptr(dY), dY.stride(0), _ptr(B), B.stride(0), dY.shape[1], _ptr(out),
+                                   _out_code(out.dtype), alpha, _stream_handle(stream)))
+        return out
+
+    def spmm_t(self, dY, out=None, out_dtype=None, alpha=1.0, beta=0.0, stream=None):
+        """dB = alpha * A^T dY + beta * out (tca_spmm_t)."""
+        torch = _torch()
+        if dY.dim() != 2 or dY.dtype != torch.float16 or dY.stride(1) != 1 or dY.shape[0] != self.M:
+            raise ValueError("dY must be an M x N float16 tensor with unit column stride")
+        out_dtype = out_dtype or (out.dtype if out is not None else torch.float32)
+        N = dY.shape[1]
+        if out is None:
+            out = torch.empty((self.K, N), dtype=out_dtype, device=dY.device)
+        _check(self._lib.tca_spmm_t(self._h, _ptr(dY), dY.stride(0), N, _ptr(out), out.stride(0),
+                                    _out_code(out.dtype), alpha, beta, _stream_handle(stream)))
+        return out
+
+    def build_transpose(self, stream=None):
+        _check(self._lib.tca_plan_build_transpose(self._h, _stream_handle(stream)))
 
     def launch_counts(self, N: int) -> tuple[int, int]:
         a, b = _I(), _I()

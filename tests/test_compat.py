@@ -1,0 +1,139 @@
+"""The drop-in boundary: the host-side I/O and conversions through the C ABI
+against the golden fixtures (CPU), and a driver written against the
+reference's C++ host API (tca-spmm_b200/examples/spmm_driver.cu) compiled and
+linked with libtca_spmm.so (CPU) and run (GPU)."""
+import ctypes
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+import tca_spmm
+
+GOLD = ROOT / "tests" / "golden"
+PKG = ROOT / "tca-spmm_b200"
+
+
+def L():
+    lib = tca_spmm.lib()
+    P = ctypes.c_void_p
+    I = ctypes.c_int
+    PP = ctypes.POINTER(ctypes.c_void_p)
+    PI = ctypes.POINTER(ctypes.c_int)
+    lib.tca_free.argtypes = [P]
+    lib.tca_free.restype = None
+    lib.tca_smtx_read.argtypes = [ctypes.c_char_p, PI, PI, PI, PP, PP, PP]
+    lib.tca_smtx_parse.argtypes = [ctypes.c_char_p, ctypes.c_size_t, PI, PI, PI, PP, PP, PP]
+    lib.tca_smtx_write.argtypes = [ctypes.c_char_p, I, I, I, P, P, P]
+    lib.tca_dense_to_csr.argtypes = [P, I, I, PI, PP, PP, PP]
+    lib.tca_csr_to_dense.argtypes = [I, I, I, P, P, P, P]
+    lib.tca_csr_to_coo.argtypes = [I, I, P, P]
+    lib.tca_coo_to_csr.argtypes = [I, I, I, P, P, P, P, P, P]
+    return lib
+
+
+def _take(lib, ptr, n, dt):
+    out = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(np.ctypeslib.as_ctypes_type(dt))),
+                                shape=(max(n, 1),))[:n].copy()
+    lib.tca_free(ptr)
+    return out
+
+
+def smtx_read(path=None, text=None):
+    lib = L()
+    M, K, nnz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rp, ci, v = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    if path is not None:
+        rc = lib.tca_smtx_read(str(path).encode(), ctypes.byref(M), ctypes.byref(K), ctypes.byref(nnz),
+                               ctypes.byref(rp), ctypes.byref(ci), ctypes.byref(v))
+    else:
+        rc = lib.tca_smtx_parse(text, len(text), ctypes.byref(M), ctypes.byref(K), ctypes.byref(nnz),
+                                ctypes.byref(rp), ctypes.byref(ci), ctypes.byref(v))
+    if rc:
+        return rc, None
+    n = nnz.value
+    return 0, (M.value, K.value, n, _take(lib, rp, M.value + 1, np.int32), _take(lib, ci, n, np.int32),
+               _take(lib, v, n, np.uint16).view(np.float16))
+
+
+@pytest.mark.parametrize("i", [0, 1, 2])
+def test_smtx_reader_matches_reference(golden, i):
+    rc, (M, K, nnz, rp, ci, v) = smtx_read(GOLD / f"smtx_{i}.smtx")
+    assert rc == 0
+    assert (M, K, nnz) == tuple(int(x) for x in golden[f"smtx_{i}_shape"])
+    rows = np.repeat(np.arange(M), np.diff(rp))
+    assert np.array_equal(np.stack([rows, ci]).astype(np.int32), golden[f"smtx_{i}_coords"])
+    assert np.all(v == 1.0)
+
+
+def test_smtx_values_line_roundtrip(tmp_path):
+    lib = L()
+    rp = np.array([0, 2, 2, 3], np.int32)
+    ci = np.array([1, 4, 0], np.int32)
+    v = np.array([0.5, -2.25, 3.0], np.float16)
+    path = tmp_path / "v.smtx"
+    assert lib.tca_smtx_write(str(path).encode(), 3, 5, 3, rp.ctypes.data, ci.ctypes.data, v.ctypes.data) == 0
+    rc, (M, K, nnz, rp2, ci2, v2) = smtx_read(path)
+    assert rc == 0 and (M, K, nnz) == (3, 5, 3)
+    assert np.array_equal(rp2, rp) and np.array_equal(ci2, ci) and np.array_equal(v2, v)
+
+
+@pytest.mark.parametrize("text", [b"3, 3\n0 1 2 3\n0 1 2\n", b"2, 2, 2\n0 1\n0 1\n", b"2, 2, 2\n0 1 2\n0 x\n",
+                                  b"2, 2, 2\n0 2 1\n0 1\n", b"2, 2, 2\n0 1 2\n0 5\n", b"1, 2, 1\n0 1\n1\n0.5 7\n"])
+def test_smtx_malformed_is_format_error(text):
+    rc, _ = smtx_read(text=text)
+    assert rc == 6
+
+
+@pytest.mark.parametrize("i", [0, 1, 2])
+def test_dense_csr_coo_conversions_match_reference(golden, i):
+    lib = L()
+    A = np.ascontiguousarray(golden[f"d2c_{i}_A"])
+    M, K = A.shape
+    nnz = ctypes.c_int()
+    rp, ci, v = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    assert lib.tca_dense_to_csr(A.ctypes.data, M, K, ctypes.byref(nnz), ctypes.byref(rp), ctypes.byref(ci),
+                                ctypes.byref(v)) == 0
+    n = nnz.value
+    rp, ci, v = _take(lib, rp, M + 1, np.int32), _take(lib, ci, n, np.int32), _take(lib, v, n, np.uint16)
+    assert np.array_equal(rp, golden[f"d2c_{i}_row_ptr"])
+    assert np.array_equal(ci, golden[f"d2c_{i}_col"])
+    assert np.array_equal(v, golden[f"d2c_{i}_val"].view(np.uint16))
+    D = np.empty((M, K), np.uint16)
+    assert lib.tca_csr_to_dense(M, K, n, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, D.ctypes.data) == 0
+    assert np.array_equal(D, golden[f"c2d_{i}_dense"].view(np.uint16))
+    # CSR -> COO -> (shuffled) -> CSR is the identity
+    ri = np.empty(n, np.int32)
+    assert lib.tca_csr_to_coo(M, n, rp.ctypes.data, ri.ctypes.data) == 0
+    perm = np.random.default_rng(i).permutation(n)
+    ri_s, ci_s, v_s = (np.ascontiguousarray(x[perm]) for x in (ri, ci, v))
+    rp2, ci2, v2 = np.empty(M + 1, np.int32), np.empty(max(n, 1), np.int32), np.empty(max(n, 1), np.uint16)
+    assert lib.tca_coo_to_csr(M, K, n, ri_s.ctypes.data, ci_s.ctypes.data, v_s.ctypes.data, rp2.ctypes.data,
+                              ci2.ctypes.data, v2.ctypes.data) == 0
+    assert np.array_equal(rp2, rp) and np.array_equal(ci2[:n], ci) and np.array_equal(v2[:n], v)
+
+
+def _build_driver(out):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    cmd = [nvcc, "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-I", str(ROOT / "include"),
+           str(PKG / "examples" / "spmm_driver.cu"), "-L", str(PKG / "lib"), "-ltca_spmm",
+           "-Xlinker", f"-rpath,{PKG / 'lib'}", "-o", str(out)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return out
+
+
+def test_reference_style_driver_compiles_and_links(tmp_path):
+    _build_driver(tmp_path / "spmm_driver")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,N", [(0, 256), (1, 64), (2, 320)])
+def test_reference_style_driver_runs(tmp_path, cuda, case, N):
+    exe = _build_driver(tmp_path / "spmm_driver")
+    r = subprocess.run([str(exe), str(GOLD / f"smtx_{case}.smtx"), str(N)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "our: [" in r.stdout
