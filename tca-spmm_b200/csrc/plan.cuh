@@ -65,6 +65,18 @@ struct tca_plan {
     struct tca_plan *tplan = nullptr;
     int *t_src = nullptr;
     __half *t_vals = nullptr;
+    // FP8-E4M3 representation of A (tca_plan_quantize_fp8): per sorted row an
+    // FP32 scale (row absmax / 448), the quantized values in sorted order, the
+    // tile entries with E4M3 bits in their low byte, and 8 KB dense images
+    // (128 x 64 bytes, 64-byte swizzled K-major) for the imaged chunks.
+    bool has_fp8 = false;
+    float *row_scale = nullptr;
+    uint8_t *p_val_f8 = nullptr;
+    uint32_t *tile_entries_f8 = nullptr;
+    uint8_t *images_f8 = nullptr;
+    // workspace of tca_spmm_fp8: B quantized per column (K x N bytes) + N scales
+    void *fp8_ws = nullptr;
+    size_t fp8_ws_bytes = 0;
 };
 
 namespace tca {
@@ -80,6 +92,16 @@ __host__ __device__ inline uint32_t swz128_offset(uint32_t r, uint32_t c)
 {
     return r * 128u + ((((c >> 3) ^ (r & 7u))) << 4) + ((c & 7u) << 1);
 }
+
+// Byte offset of element (r, c) of a 128 x 64 one-byte (E4M3) tile in the
+// 64-byte swizzled K-major layout: 16-byte chunk index c/16 XOR-ed with
+// (r / 2) % 4 (address bits 4-5 XOR bits 7-8).
+__host__ __device__ inline uint32_t swz64_offset(uint32_t r, uint32_t c)
+{
+    return r * 64u + ((((c >> 4) ^ ((r >> 1) & 3u))) << 4) + (c & 15u);
+}
+
+constexpr float kE4M3Max = 448.f;
 
 // Largest K for which windows may go to the tensor-core path: the builder
 // keeps a K-bit column bitmap plus its prefix counts in shared memory.
