@@ -17,8 +17,11 @@
 //
 // Malformed CSR never faults: row ranges are clamped to [0, nnz] and
 // nonzeros whose column is outside [0, K) contribute nothing.
+#include <algorithm>
+#include <vector>
 #include "tca_internal.cuh"
 #include "plan.cuh"
+#include "ptx.cuh"
 
 namespace tca {
 namespace {
@@ -245,7 +248,8 @@ struct CcJob {
 
 struct CcBatch {
     int n_jobs;
-    int block_start[kMaxCcJobs + 1];
+    int block_start[kMaxCcJobs + 1]; // first block of each job (spmm_cc_items_kernel)
+    int item_start[kMaxCcJobs + 1];  // first item of each job in the flattened list (spmm_cc_stream_kernel)
     CcJob job[kMaxCcJobs];
 };
 
@@ -349,6 +353,213 @@ __global__ void __launch_bounds__(256) spmm_cc_items_kernel(const __grid_constan
     }
 }
 
+// ---------------------------------------------------------------------------
+// Vectorised item stream: one warp per stream of items, persistent.
+//
+// Warp w takes items w, w + n_warps, ... of the flattened item list of all
+// jobs. Each item's metadata is fetched by a three-deep software pipeline so
+// that no dependent load chain is exposed between items: while item i is
+// computed, the nonzeros (column, value) of item i+1, the row offsets and
+// output rows of item i+2 and the descriptor of item i+3 are in flight.
+// Lane k holds row offset k and output row k of its item and nonzero k of its
+// first 32; every lane owns W consecutive output columns (W halves of B per
+// load, 8 loads in flight per lane) and accumulates with mixed-precision FMA
+// (FP16 x FP16 + FP32, one rounding -- the same value as converting both
+// factors to FP32 and using fmaf).
+// ---------------------------------------------------------------------------
+template <int W> struct HalfVec;
+template <> struct HalfVec<8> { using T = uint4; };
+template <> struct HalfVec<4> { using T = uint2; };
+template <> struct HalfVec<2> { using T = unsigned; };
+
+using ptx::fma_f16_f32;
+
+template <int W> __device__ __forceinline__ void load_out(const __half *p, float *v)
+{
+    using V = typename HalfVec<W>::T;
+    const V u = *reinterpret_cast<const V *>(p);
+    const __half *h = reinterpret_cast<const __half *>(&u);
+#pragma unroll
+    for (int i = 0; i < W; i++) v[i] = __half2float(h[i]);
+}
+template <int W> __device__ __forceinline__ void load_out(const float *p, float *v)
+{
+#pragma unroll
+    for (int i = 0; i < W; i += 2) {
+        const float2 f = reinterpret_cast<const float2 *>(p)[i / 2];
+        v[i] = f.x;
+        v[i + 1] = f.y;
+    }
+}
+template <int W> __device__ __forceinline__ void store_out(__half *p, const float *v)
+{
+    using V = typename HalfVec<W>::T;
+    V u;
+    __half2 *h = reinterpret_cast<__half2 *>(&u);
+#pragma unroll
+    for (int i = 0; i < W / 2; i++) h[i] = __floats2half2_rn(v[2 * i], v[2 * i + 1]);
+    *reinterpret_cast<V *>(p) = u;
+}
+template <int W> __device__ __forceinline__ void store_out(float *p, const float *v)
+{
+    if constexpr (W >= 4) {
+#pragma unroll
+        for (int i = 0; i < W; i += 4)
+            reinterpret_cast<float4 *>(p)[i / 4] = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+    } else {
+        *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+    }
+}
+
+struct ItemDesc {
+    int job, r0, nrows; // nrows == 0: no item
+};
+
+__device__ __forceinline__ ItemDesc load_desc(const CcBatch &b, int item)
+{
+    ItemDesc d{0, 0, 0};
+    if (item < b.item_start[b.n_jobs]) {
+        int j = 0;
+        while (j + 1 < b.n_jobs && b.item_start[j + 1] <= item) j++;
+        const int2 it = __ldg(b.job[j].items + (item - b.item_start[j]));
+        d.job = j;
+        d.r0 = it.x;
+        d.nrows = it.y - it.x;
+    }
+    return d;
+}
+
+template <typename OutT, int W>
+__global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(const __grid_constant__ CcBatch b)
+{
+    using V = typename HalfVec<W>::T;
+    constexpr int U = 8;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int n_warps = (int)gridDim.x * 8;
+    int item = (int)blockIdx.x * 8 + (int)(threadIdx.x >> 5);
+
+    // row offsets (lane k <= nrows) and output rows (lane k < nrows) of an item
+    auto load_rows = [&](const ItemDesc &d, int &rs, int &orow) {
+        rs = 0;
+        orow = 0;
+        if (lane <= d.nrows && d.nrows > 0) {
+            const CcJob &a = b.job[d.job];
+            rs = __ldg(a.p_row_ptr + d.r0 + lane);
+            if (lane < d.nrows)
+                orow = __ldg(a.perm + d.r0 + lane);
+        }
+    };
+    // the item's first 32 nonzeros, one per lane
+    auto load_nz = [&](const ItemDesc &d, int rs, int &col, unsigned short &val) {
+        const int j0 = __shfl_sync(full, rs, 0), j1 = __shfl_sync(full, rs, d.nrows & 31);
+        col = 0;
+        val = 0;
+        if (d.nrows > 0 && j0 + lane < j1) {
+            const CcJob &a = b.job[d.job];
+            col = __ldg(a.p_col + j0 + lane);
+            val = __half_as_ushort(a.p_val[j0 + lane]);
+        }
+    };
+
+    ItemDesc d0 = load_desc(b, item), d1 = load_desc(b, item + n_warps), d2 = load_desc(b, item + 2 * n_warps);
+    int rs0, out0, rs1, out1, col0;
+    unsigned short val0;
+    load_rows(d0, rs0, out0);
+    load_rows(d1, rs1, out1);
+    load_nz(d0, rs0, col0, val0);
+
+    while (d0.nrows > 0) {
+        // ---- pipeline: nonzeros of i+1, rows of i+2, descriptor of i+3
+        int col1;
+        unsigned short val1;
+        load_nz(d1, rs1, col1, val1);
+        int rs2, out2;
+        load_rows(d2, rs2, out2);
+        const ItemDesc d3 = load_desc(b, item + 3 * n_warps);
+
+        // ---- item i
+        const CcJob &a = b.job[d0.job];
+        const int nrows = d0.nrows;
+        const int j0 = __shfl_sync(full, rs0, 0), j1 = __shfl_sync(full, rs0, nrows);
+        const bool keep = (a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) != 0;
+        for (int nb = 0; nb < a.N; nb += 32 * W) {
+            const int n0 = nb + lane * W;
+            const bool active = n0 < a.N;
+            const __half *Bn = a.B + (active ? n0 : 0);
+            float acc[W];
+#pragma unroll
+            for (int i = 0; i < W; i++) acc[i] = 0.f;
+            int cr = 0;
+            int ce = __shfl_sync(full, rs0, 1);
+            auto flush = [&]() {
+                const int rstart = __shfl_sync(full, rs0, cr);
+                const int orow = __shfl_sync(full, out0, cr);
+                if (active && !(keep && rstart == ce)) {
+                    OutT *cp = reinterpret_cast<OutT *>(a.C) + (size_t)orow * a.ldc + n0;
+                    float o[W];
+                    if (a.beta != 0.f) {
+                        float old[W];
+                        load_out<W>(cp, old);
+#pragma unroll
+                        for (int i = 0; i < W; i++) o[i] = fmaf(a.alpha, acc[i], a.beta * old[i]);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < W; i++) o[i] = a.alpha * acc[i];
+                    }
+                    store_out<W>(cp, o);
+                }
+#pragma unroll
+                for (int i = 0; i < W; i++) acc[i] = 0.f;
+                cr++;
+                const int nxt = __shfl_sync(full, rs0, min(cr + 1, 31));
+                ce = cr < nrows ? nxt : 0x7fffffff;
+            };
+            for (int base = j0; base < j1; base += 32) {
+                int c = col0;
+                unsigned short v = val0;
+                if (base != j0) { // a row longer than 32 nonzeros: the rest is loaded here
+                    c = 0;
+                    v = 0;
+                    if (base + lane < j1) {
+                        c = __ldg(a.p_col + base + lane);
+                        v = __half_as_ushort(a.p_val[base + lane]);
+                    }
+                }
+                const int m = min(32, j1 - base);
+                for (int t = 0; t < m; t += U) {
+                    V bv[U];
+                    unsigned short av[U];
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        const int cu = __shfl_sync(full, c, t + u);
+                        av[u] = (unsigned short)__shfl_sync(full, (int)v, t + u);
+                        bv[u] = V{};
+                        if (active && t + u < m)
+                            bv[u] = __ldg(reinterpret_cast<const V *>(Bn + (size_t)cu * a.ldb));
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        if (t + u < m) { // uniform across the warp
+                            while (base + t + u >= ce) flush();
+                            const unsigned short *h = reinterpret_cast<const unsigned short *>(&bv[u]);
+#pragma unroll
+                            for (int i = 0; i < W; i++) acc[i] = fma_f16_f32(av[u], h[i], acc[i]);
+                        }
+                    }
+                }
+            }
+            while (cr < nrows) flush();
+        }
+
+        // ---- rotate the pipeline
+        d0 = d1; rs0 = rs1; out0 = out1; col0 = col1; val0 = val1;
+        d1 = d2; rs1 = rs2; out1 = out2;
+        d2 = d3;
+        item += n_warps;
+    }
+}
+
 template <typename OutT, int LPR>
 void launch_vec(const int *rp, const int *ci, const __half *v, int M, int K, int nnz, const __half *B, int ldb,
                 int N, OutT *C, int ldc, float alpha, float beta, unsigned flags, cudaStream_t s)
@@ -419,15 +630,37 @@ int launch_cc_group(const CcBatch &b, cudaStream_t s)
     return TCA_OK;
 }
 
+// Persistent grid of the stream kernel: enough warps for every item, at most
+// the resident blocks of all SMs.
+template <typename OutT, int W>
+int launch_stream_group(const CcBatch &b, cudaStream_t s)
+{
+    const int total = b.item_start[b.n_jobs];
+    if (b.n_jobs == 0 || total == 0)
+        return TCA_OK;
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        int n = 0;
+        TCA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spmm_cc_stream_kernel<OutT, W>, 256, 0));
+        per_sm = n > 0 ? n : 1;
+    }
+    const int grid = std::min((total + 7) / 8, kSMs * per_sm);
+    spmm_cc_stream_kernel<OutT, W><<<grid, 256, 0, s>>>(b);
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
+// Columns per lane of the stream kernel: 8 for N > 128, 4 for N > 64, else 2.
+inline int pick_w(int N) { return N > 128 ? 8 : N > 64 ? 4 : 2; }
+
 template <typename OutT>
-int launch_cc_typed(const CcBatch &b, int lpr, bool vec, cudaStream_t s)
+int launch_cc_typed(const CcBatch &b, int w, bool vec, cudaStream_t s)
 {
     if (!vec) return launch_cc_group<OutT, 32, false>(b, s);
-    switch (lpr) {
-    case 4: return launch_cc_group<OutT, 4, true>(b, s);
-    case 8: return launch_cc_group<OutT, 8, true>(b, s);
-    case 16: return launch_cc_group<OutT, 16, true>(b, s);
-    default: return launch_cc_group<OutT, 32, true>(b, s);
+    switch (w) {
+    case 2: return launch_stream_group<OutT, 2>(b, s);
+    case 4: return launch_stream_group<OutT, 4>(b, s);
+    default: return launch_stream_group<OutT, 8>(b, s);
     }
 }
 
@@ -436,12 +669,13 @@ int launch_cc_typed(const CcBatch &b, int lpr, bool vec, cudaStream_t s)
 int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
                    cudaStream_t s)
 {
-    // groups: (lanes per row, vectorised) -- 4/8/16/32 x vec, plus scalar
-    const int kinds[5][2] = {{4, 1}, {8, 1}, {16, 1}, {32, 1}, {32, 0}};
+    // groups: (columns per lane, vectorised) -- stream kernel with 2/4/8 columns, plus scalar items
+    const int kinds[4][2] = {{2, 1}, {4, 1}, {8, 1}, {32, 0}};
     for (const auto &kd : kinds) {
         CcBatch b;
         b.n_jobs = 0;
         b.block_start[0] = 0;
+        b.item_start[0] = 0;
         auto flush = [&]() -> int {
             const int st = (c_dtype == TCA_DTYPE_F16) ? launch_cc_typed<__half>(b, kd[0], kd[1] != 0, s)
                                                       : launch_cc_typed<float>(b, kd[0], kd[1] != 0, s);
@@ -455,7 +689,7 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
             if (n_items == 0 || sj.N <= 0)
                 continue;
             const bool vec = vec_ok(sj.B, sj.ldb, sj.N, sj.C, sj.ldc, c_dtype);
-            const int lpr = vec ? pick_lpr(sj.N) : 32;
+            const int lpr = vec ? pick_w(sj.N) : 32;
             if (lpr != kd[0] || (vec ? 1 : 0) != kd[1])
                 continue;
             CcJob &a = b.job[b.n_jobs];
@@ -475,8 +709,9 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
             a.alpha = alpha;
             a.beta = beta;
             a.flags = flags;
-            const int per_block = 256 / lpr;
+            const int per_block = vec ? 8 : 256 / lpr;
             b.block_start[b.n_jobs + 1] = b.block_start[b.n_jobs] + (a.n_items + per_block - 1) / per_block;
+            b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + a.n_items;
             b.n_jobs++;
             if (b.n_jobs == kMaxCcJobs)
                 TCA_TRY(flush());

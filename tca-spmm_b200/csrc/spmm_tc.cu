@@ -9,15 +9,18 @@
 // tile multiplies the 64 matching rows of B on the 5th-generation tensor
 // cores: D[128 x NT] (FP32, tensor memory) += A[128 x 64] * B[64 x NT].
 //
-// One CTA = one (job, window, NT-wide slice of N) work item, a ring of
-// kStages (A tile, B tile, entry staging) stages and three decoupled roles:
-//   * one loader warp moves every byte through the TMA engine: the 64 B rows
-//     of the chunk's condensed columns by tile::gather4 (4 rows x 128 bytes
-//     per instruction into a 128-byte swizzled N-major tile; padding columns
-//     and n >= N are out of the tensor and arrive as zeros), and either the
-//     chunk's pre-rendered, pre-swizzled dense A tile (chunks with >= 2048
-//     nonzeros: one 16 KB cp.async.bulk) or its packed entries (cp.async.bulk
-//     into the stage's staging buffer);
+// Work items are (job, window, NT-wide slice of N); persistent CTAs (one per
+// SM) stream the chunks of their items through a ring of kStages (A tile,
+// B tile, entry staging) stages, with decoupled roles:
+//   * four loader warps, taking chunks in turn, move every byte through the
+//     TMA engine: the 64 B rows of the chunk -- one tiled box per 64 columns
+//     of N when its columns are 64 consecutive rows of B, else tile::gather4
+//     of the condensed columns (4 rows x 128 bytes per instruction into a
+//     128-byte swizzled N-major tile; padding columns and n >= N are out of
+//     the tensor and arrive as zeros) -- and either the chunk's pre-rendered,
+//     pre-swizzled dense A tile (chunks with >= 2048 nonzeros: one 16 KB
+//     cp.async.bulk) or its packed entries (cp.async.bulk into the stage's
+//     staging buffer);
 //   * scatter warps, once a stage's entries landed, zero its A tile and
 //     scatter them into the 128-byte swizzled K-major layout;
 //   * one MMA lane issues 4 tcgen05.mma (K = 16 each) per chunk into the FP32
@@ -36,17 +39,18 @@
 #include <mutex>
 #include "tca_internal.cuh"
 #include "plan.cuh"
+#include "ptx.cuh"
 
 namespace tca {
 namespace {
 
 constexpr int kScatterThreads = 128; // warps 0-3: sparse-entry scatter
-constexpr int kLoaderWarp = 4;       // TMA issue
+constexpr int kLoaderWarp = 4;       // TMA issue, chunks g = 0 (mod kLoaders)
 constexpr int kMmaWarp = 5;          // TMEM allocation, tcgen05.mma issue
 constexpr int kEpiThreads = 128;     // warps 6-9: epilogue
-constexpr int kThreads = 320;
-constexpr int kMetaRing = 8;          // chunk-metadata prefetch ring (prefetch distance kMetaRing - 1)
-constexpr int kMetaSlotInts = 68;     // 64 columns, image index, first and end entry, pad
+constexpr int kLoaderWarp1 = 10;     // warps 10..: TMA issue, chunks g = 1, 2, .. (mod kLoaders)
+constexpr int kLoaders = 4;          // loader warps, each issuing every kLoaders-th chunk
+constexpr int kThreads = 320 + (kLoaders - 1) * 32;
 constexpr int kMaxCtaItems = 32;      // work items per persistent CTA
 constexpr int kATileBytes = kWindowRows * kChunkCols * 2;     // 16 KB
 constexpr int kStagingBytes = ((kImageMinNnz + 3) * 4 + 15) & ~15; // entries of a sparse chunk, 16-byte rounded
@@ -73,105 +77,7 @@ struct TcBatch {
     TcJob job[kMaxJobs];
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}\n"
-                 : "=r"(ok)
-                 : "r"(smem_u32(bar)), "r"(parity)
-                 : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns()
-{
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// Bounded wait for the phase of `parity`: false after about one second.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
-{
-    if (mbar_try_wait(bar, parity))
-        return true;
-    const uint64_t t0 = global_ns();
-    for (uint32_t it = 1;; ++it) {
-        if (mbar_try_wait(bar, parity))
-            return true;
-        if ((it & 255u) == 0u && global_ns() - t0 > 1000000000ull)
-            return false;
-    }
-}
-
-__device__ __forceinline__ void named_bar_sync(int id, int n)
-{
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-// 1-D bulk copy global -> this CTA's shared memory, completing on `bar`.
-__device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-// mbarrier arrive (count 1) that also adds `bytes` to the transaction count.
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// TMA gather of 4 rows (y0..y3) x one 64-element box starting at column x of a
-// 2-D tensor into shared memory, completing on `bar`. Rows or columns outside
-// the tensor are zero-filled.
-__device__ __forceinline__ void tma_gather4(uint32_t dst, const CUtensorMap *map, int x, int y0, int y1, int y2,
-                                            int y3, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
-                 " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(dst),
-                 "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y0), "r"(y1), "r"(y2), "r"(y3)
-                 : "memory");
-}
-
-// TMA load of a {64 columns x 64 rows} box of a 2-D tensor at (x, y) into
-// shared memory, completing on `bar`; out-of-range elements are zero-filled.
-__device__ __forceinline__ void tma_tile2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-                 " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
-                 "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// Shared-memory matrix descriptor, 128-byte swizzle (layout type 2), version 1.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
-{
-    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (2ull << 61);
-}
+using namespace ptx;
 
 // kind::f16 instruction descriptor: D FP32, A/B FP16, A K-major, B N-major, M = 128.
 __host__ __device__ constexpr uint32_t idesc_f16(int n)
@@ -188,23 +94,6 @@ __device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b
                  "l"(a), "l"(b), "r"(idesc), "r"(accum)
                  : "memory");
 }
-__device__ __forceinline__ void umma_commit(uint64_t *bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t *r)
-{
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-                   "=r"(r[14]), "=r"(r[15])
-                 : "r"(addr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
 __device__ __forceinline__ void store8_out(__half *p, const float *v, float alpha, float beta)
 {
     uint4 u;
@@ -240,8 +129,8 @@ __device__ __forceinline__ void store8_out(float *p, const float *v, float alpha
 }
 
 // Shared memory (1024-byte aligned base): kStages x (A tile | B tile),
-// kStages entry staging buffers, per-stage chunk records, the chunk-metadata
-// ring, the CTA's item table, mbarriers and two broadcast flags + TMEM slot.
+// kStages entry staging buffers, per-stage chunk records, the CTA's item
+// table, mbarriers and two broadcast flags + TMEM slot.
 template <int NT> struct TcCfg {
     static constexpr int kStages = NT == 256 ? 4 : NT == 128 ? 5 : 6;
     static constexpr int kBTileBytes = kChunkCols * NT * 2;
@@ -249,27 +138,16 @@ template <int NT> struct TcCfg {
     static constexpr int kStagingOff = kStages * kStage;
     static constexpr int kPendOff = kStagingOff + kStages * kStagingBytes; // int4 [kStages]: img, e0, e0a, e1
     static constexpr int kPend2Off = kPendOff + kStages * 16;              // int4 [kStages]: flags, buffer, item
-    static constexpr int kMetaOff = kPend2Off + kStages * 16;              // int [kMetaRing][kMetaSlotInts]
-    static constexpr int kItemOff = kMetaOff + kMetaRing * kMetaSlotInts * 4; // int4 [kMaxCtaItems]
+    static constexpr int kItemOff = kPend2Off + kStages * 16;              // int4 [kMaxCtaItems]
     static constexpr int kBarOff = kItemOff + kMaxCtaItems * 16;
     // full, empty, staged [kStages]; accum_full, accum_empty [2]
     static constexpr int kSmem = kBarOff + (3 * kStages + 4) * 8 + 16;
     static_assert(kSmem <= 227 * 1024, "shared memory budget");
     static_assert(kStage % 1024 == 0 && kATileBytes % 1024 == 0, "swizzled tiles need 1024-byte alignment");
     static_assert(kStagingOff % 16 == 0 && kStagingBytes % 16 == 0 && kPendOff % 16 == 0, "16-byte alignment");
-    static_assert(kMetaOff % 16 == 0 && kItemOff % 16 == 0 && kBarOff % 16 == 0, "16-byte aligned regions");
+    static_assert(kItemOff % 16 == 0 && kBarOff % 16 == 0, "16-byte aligned regions");
+    static_assert(kLoaders <= kStages, "a loader may not lap a stage that an earlier loader still fills");
 };
-
-__device__ __forceinline__ void cp_async4(uint32_t dst, const void *src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Work item (job, tensor-core window, N slice) -> table entry {window,
 // first chunk, chunk count, job << 16 | N-slice index}.
@@ -285,16 +163,20 @@ __device__ __forceinline__ int4 decode_item(const TcBatch &batch, int item)
 
 // Persistent CTAs, one per SM: CTA b processes work items b, b + gridDim.x,
 // ... (at most kMaxCtaItems), as one continuous stream of chunks through the
-// stage ring. Warp roles (320 threads):
-//   warp 4 (loader): per chunk, acquire the stage ("empty"), write the
+// stage ring. Warp roles (kThreads threads):
+//   warps 4, 10, 11, 12 (loaders; loader l takes chunks g = l (mod kLoaders),
+//     so that four chunks are being issued at once -- one warp issuing every
+//     chunk in turn was measured to need ~0.9 us per chunk, three times the
+//     tensor-core time of an N = 256 chunk): per chunk, acquire the stage ("empty"), write the
 //     chunk's records (entries range and image for the scatter warps; first /
 //     last chunk of its item and accumulator buffer for the MMA lane), set the
 //     "full" transaction count and issue the dense A image (16 KB
 //     cp.async.bulk) or the sparse entries (cp.async.bulk into staging,
 //     completing on "staged"), then the B rows: tiled TMA boxes of 64
 //     contiguous rows for direct chunks, tile::gather4 for condensed ones.
-//     Chunk metadata is prefetched kMetaRing - 1 chunks ahead with cp.async.
-//     After the last chunk it passes an end record through the ring.
+//     Chunk metadata (columns, image, entry range) is loaded into registers
+//     one chunk of the same loader ahead. The loader owning position
+//     total_chunks passes an end record through the ring.
 //   warps 0-3 (scatter): per chunk, wait "staged"; for a sparse chunk zero the
 //     A tile, scatter the staged entries, fence.proxy.async; arrive "full".
 //   warp 5, lane 0 (MMA): per chunk wait "full"; on an item's first chunk
@@ -311,11 +193,9 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     constexpr int S = Cfg::kStages;
     constexpr int kBoxes = NT / 64;       // 64-column boxes per B row slice
     constexpr int kGathers = 16 * kBoxes; // gather4 instructions per condensed chunk
-    constexpr int P = kMetaRing - 1;      // metadata prefetch distance
     extern __shared__ __align__(1024) uint8_t smem[];
     int4 *pend = reinterpret_cast<int4 *>(smem + Cfg::kPendOff);
     int4 *pend2 = reinterpret_cast<int4 *>(smem + Cfg::kPend2Off);
-    int *meta = reinterpret_cast<int *>(smem + Cfg::kMetaOff);
     int4 *items = reinterpret_cast<int4 *>(smem + Cfg::kItemOff);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + Cfg::kBarOff);
     uint64_t *empty = full + S;
@@ -359,81 +239,97 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
 
-    if (warp == kLoaderWarp) {
-        // ---------------- loader ----------------
-        // prefetch cursor: (item k, chunk i) of the next chunk whose metadata to fetch
-        int pk = 0, pi = 0;
-        auto prefetch = [&](int slot) {
-            if (pk < n_items) {
-                const int4 it = items[pk];
-                const TcJob &a = batch.job[it.w >> 16];
-                const int c = it.y + pi;
-                const uint32_t dst = smem_u32(meta + slot * kMetaSlotInts);
-                if (lane < 16)
-                    cp_async16(dst + lane * 16, a.win_cols + (size_t)c * kChunkCols + lane * 4);
-                else if (lane == 16)
-                    cp_async4(dst + 64 * 4, a.img_idx + c);
-                else if (lane == 17)
-                    cp_async4(dst + 65 * 4, a.tile_ptr + c);
-                else if (lane == 18)
-                    cp_async4(dst + 66 * 4, a.tile_ptr + c + 1);
-                if (++pi == it.z) { pi = 0; pk++; }
-            }
-            cp_async_commit();
+    if (warp == kLoaderWarp || warp >= kLoaderWarp1) {
+        // ---------------- loaders ----------------
+        // Loader ld issues chunks g = ld, ld + kLoaders, ... of the CTA's chunk
+        // stream; (k, i) is the item and chunk-within-item of its next chunk.
+        const int ld = warp == kLoaderWarp ? 0 : warp - kLoaderWarp1 + 1;
+        int total_chunks = 0;
+        for (int k = 0; k < n_items; k++) total_chunks += items[k].z;
+        auto advance = [&](int &k, int &i) {
+            while (k < n_items && i >= items[k].z) { i -= items[k].z; k++; }
         };
-        for (int q = 0; q < P; q++) prefetch(q);
-        int g = 0;
-        for (int k = 0; k < n_items && ok; k++) {
+        // per-chunk metadata in registers: lanes 0-15 hold 4 columns each, every
+        // lane the image index and entry range; fetched one chunk of this loader ahead
+        struct Meta { int4 cols; int img, e0, e1; };
+        auto fetch = [&](int k, int i, Meta &m) {
+            m.cols = make_int4(-1, -1, -1, -1);
+            m.img = -1;
+            m.e0 = m.e1 = 0;
+            if (k < n_items) {
+                const int4 it = items[k];
+                const TcJob &a = batch.job[it.w >> 16];
+                const int c = it.y + i;
+                if (lane < 16)
+                    m.cols = __ldg(reinterpret_cast<const int4 *>(a.win_cols + (size_t)c * kChunkCols) + lane);
+                m.img = __ldg(a.img_idx + c);
+                m.e0 = __ldg(a.tile_ptr + c);
+                m.e1 = __ldg(a.tile_ptr + c + 1);
+            }
+        };
+        int k = 0, i = ld;
+        advance(k, i);
+        Meta cur, nxt;
+        fetch(k, i, cur);
+        int g = ld;
+        for (; g < total_chunks; g += kLoaders) {
+            int k2 = k, i2 = i + kLoaders;
+            advance(k2, i2);
+            fetch(k2, i2, nxt); // in flight while this chunk's stage is acquired and issued
+            const int s = g % S;
+            uint32_t got = 1;
+            if (lane == 0 && g >= S)
+                got = mbar_wait(&empty[s], ((g / S) - 1) & 1) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) { ok = false; break; }
             const int4 it = items[k];
             const TcJob &a = batch.job[it.w >> 16];
             const int n0 = (it.w & 0xffff) * NT;
-            for (int i = 0; i < it.z; i++, g++) {
-                const int s = g % S;
-                uint32_t got = 1;
-                if (lane == 0 && g >= S)
-                    got = mbar_wait(&empty[s], ((g / S) - 1) & 1) ? 1u : 0u;
-                got = __shfl_sync(0xffffffffu, got, 0);
-                if (!got) { ok = false; break; }
-                cp_async_wait<P - 1>(); // this chunk's metadata has landed (this lane's share)
-                __syncwarp();           // ... and every lane's
-                const int *m = meta + (g % kMetaRing) * kMetaSlotInts;
-                const int img = m[64];
-                const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
-                if (lane == 0) {
-                    const int e0 = m[65], e1 = m[66], e0a = e0 & ~3;
-                    pend[s] = make_int4(img, e0, e0a, e1);
-                    pend2[s] = make_int4((i == 0 ? 1 : 0) | (i == it.z - 1 ? 2 : 0), k & 1, k, 0);
-                    mbar_expect_tx(&full[s], Cfg::kBTileBytes + (img >= 0 ? kATileBytes : 0));
-                    if (img >= 0) {
-                        bulk_copy_g2s(a_s, a.images + (size_t)img * (kATileBytes / 2), kATileBytes, &full[s]);
-                        mbar_arrive(&staged[s]);
-                    } else if (e1 > e0) {
-                        const uint32_t bytes = (uint32_t)(((e1 - e0a) * 4 + 15) & ~15);
-                        mbar_arrive_expect_tx(&staged[s], bytes);
-                        bulk_copy_g2s(smem_u32(smem + Cfg::kStagingOff + s * kStagingBytes), a.entries + e0a, bytes,
-                                      &staged[s]);
-                    } else {
-                        mbar_arrive(&staged[s]);
-                    }
-                }
-                __syncwarp(); // the transaction count is set before any B load is issued
-                if (m[0] >= 0 && m[kChunkCols - 1] == m[0] + kChunkCols - 1) {
-                    // 64 contiguous B rows (direct chunks): one 8 KB tiled box per 64 columns
-                    if (lane < kBoxes)
-                        tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * 64, m[0], &full[s]);
+            const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
+            if (lane == 0) {
+                const int img = cur.img, e0 = cur.e0, e1 = cur.e1, e0a = e0 & ~3;
+                pend[s] = make_int4(img, e0, e0a, e1);
+                pend2[s] = make_int4((i == 0 ? 1 : 0) | (i == it.z - 1 ? 2 : 0), k & 1, k, 0);
+                mbar_expect_tx(&full[s], Cfg::kBTileBytes + (img >= 0 ? kATileBytes : 0));
+                if (img >= 0) {
+                    bulk_copy_g2s(a_s, a.images + (size_t)img * (kATileBytes / 2), kATileBytes, &full[s]);
+                    mbar_arrive(&staged[s]);
+                } else if (e1 > e0) {
+                    const uint32_t bytes = (uint32_t)(((e1 - e0a) * 4 + 15) & ~15);
+                    mbar_arrive_expect_tx(&staged[s], bytes);
+                    bulk_copy_g2s(smem_u32(smem + Cfg::kStagingOff + s * kStagingBytes), a.entries + e0a, bytes,
+                                  &staged[s]);
                 } else {
-                    for (int q = lane; q < kGathers; q += 32) {
-                        const int gg = q & 15, box = q >> 4;
-                        tma_gather4(b_s + box * (kChunkCols * 128) + gg * 512, &a.tmap_b, n0 + box * 64, m[4 * gg],
-                                    m[4 * gg + 1], m[4 * gg + 2], m[4 * gg + 3], &full[s]);
-                    }
+                    mbar_arrive(&staged[s]);
                 }
-                __syncwarp(); // every lane has read slot g before it is refilled
-                prefetch((g + P) % kMetaRing);
             }
+            __syncwarp(); // the transaction count is set before any B load is issued
+            const int col0 = __shfl_sync(0xffffffffu, cur.cols.x, 0);
+            const int col63 = __shfl_sync(0xffffffffu, cur.cols.w, 15);
+            if (col0 >= 0 && col63 == col0 + kChunkCols - 1) {
+                // 64 contiguous B rows (direct chunks): one 8 KB tiled box per 64 columns
+                if (lane < kBoxes)
+                    tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * 64, col0, &full[s]);
+            } else {
+                // condensed columns: gather q = lane, lane + 32, .. reads the 4 columns of lane q % 16
+                const int src = lane & 15;
+                const int y0 = __shfl_sync(0xffffffffu, cur.cols.x, src);
+                const int y1 = __shfl_sync(0xffffffffu, cur.cols.y, src);
+                const int y2 = __shfl_sync(0xffffffffu, cur.cols.z, src);
+                const int y3 = __shfl_sync(0xffffffffu, cur.cols.w, src);
+                for (int q = lane; q < kGathers; q += 32) {
+                    const int box = q >> 4;
+                    tma_gather4(b_s + box * (kChunkCols * 128) + src * 512, &a.tmap_b, n0 + box * 64, y0, y1, y2, y3,
+                                &full[s]);
+                }
+            }
+            cur = nxt;
+            k = k2;
+            i = i2;
         }
-        // end record: scatter warps and the MMA lane stop at it
-        if (ok) {
+        // end record (written by the loader that owns chunk position total_chunks):
+        // the scatter warps and the MMA lane stop at it
+        if (ok && g == total_chunks) {
             const int s = g % S;
             uint32_t got = 1;
             if (lane == 0 && g >= S)
@@ -445,7 +341,6 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             }
             if (!got) ok = false;
         }
-        cp_async_wait<0>();
     } else if (warp < 4) {
         // ---------------- scatter ----------------
         const int sid = threadIdx.x;
@@ -562,23 +457,36 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
-// B (K x N, row-major, leading dimension ldb) as a TMA source: dims {N, K},
-// row stride ldb * 2 bytes, box {64, rows}, 128-byte swizzle, zero fill.
-int encode_b_map(const SpmmJob &sj, int K, int rows, CUtensorMap *map)
+} // namespace
+
+int encode_tensor_map_2d(CUtensorMap *map, CUtensorMapDataType dtype, const void *base, uint64_t d0, uint64_t d1,
+                         uint64_t row_stride_bytes, uint32_t b0, uint32_t b1, CUtensorMapSwizzle swizzle)
 {
     auto enc = tensor_map_encoder();
     if (!enc)
         return set_error(TCA_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    const cuuint64_t dims[2] = {(cuuint64_t)sj.N, (cuuint64_t)(K > 0 ? K : 1)};
-    const cuuint64_t strides[1] = {(cuuint64_t)sj.ldb * 2};
-    const cuuint32_t box[2] = {64, (cuuint32_t)rows};
+    const cuuint64_t dims[2] = {(cuuint64_t)d0, (cuuint64_t)(d1 > 0 ? d1 : 1)};
+    const cuuint64_t strides[1] = {(cuuint64_t)row_stride_bytes};
+    const cuuint32_t box[2] = {b0, b1};
     const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<__half *>(sj.B), dims, strides, box,
-                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const CUresult r = enc(map, dtype, 2, const_cast<void *>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
-        return set_error(TCA_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d) for B (N=%d, ldb=%d)", (int)r, sj.N, sj.ldb);
+        return set_error(TCA_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d): dims {%llu, %llu}, stride %llu, box {%u, %u}",
+                         (int)r, (unsigned long long)d0, (unsigned long long)d1, (unsigned long long)row_stride_bytes,
+                         b0, b1);
     return TCA_OK;
+}
+
+namespace {
+
+// B (K x N, row-major, leading dimension ldb) as a TMA source: dims {N, K},
+// row stride ldb * 2 bytes, box {64, rows}, 128-byte swizzle, zero fill.
+int encode_b_map(const SpmmJob &sj, int K, int rows, CUtensorMap *map)
+{
+    return encode_tensor_map_2d(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, sj.B, (uint64_t)sj.N, (uint64_t)K,
+                                (uint64_t)sj.ldb * 2, 64, (uint32_t)rows, CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
 int make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT, TcJob *out)
