@@ -119,7 +119,11 @@ typedef enum tca_plan_array {
     TCA_ARR_TILE_IMAGE_IDX = 12, /* [int, n_tc_chunks] dense image of each chunk, -1 = none */
     TCA_ARR_TILE_IMAGES = 13, /* [fp16, n_images*8192] dense 128x64 tiles, 128-byte swizzled K-major */
     TCA_ARR_CC_ITEMS = 14,    /* [int pairs] CUDA-core items [first, end) of sorted rows, CUDA-core windows */
-    TCA_ARR_ALL_ITEMS = 15    /* [int pairs] the same over all windows */
+    TCA_ARR_ALL_ITEMS = 15,   /* [int pairs] the same over all windows */
+    TCA_ARR_ROW_SCALE = 16,   /* [float, M] E4M3 scale per sorted row (after tca_plan_quantize_fp8) */
+    TCA_ARR_P_VAL_F8 = 17,    /* [u8, nnz] E4M3 values, sorted order */
+    TCA_ARR_TILE_ENTRIES_F8 = 18, /* [u32] tile entries with the E4M3 value in the low byte */
+    TCA_ARR_TILE_IMAGES_F8 = 19   /* [u8, n_images*8192] dense 128x64 E4M3 tiles, 64-byte swizzled K-major */
 } tca_plan_array_t;
 
 TCA_API void tca_plan_opts_default(tca_plan_opts_t *opts);
@@ -194,6 +198,32 @@ TCA_API int tca_plan_build_transpose(tca_plan_t plan, tca_stream_t stream);
 /* How many tensor-core and CUDA-core kernel launches one tca_spmm with this
  * N makes (0 or 1 each). */
 TCA_API int tca_plan_launch_counts(tca_plan_t plan, int N, int *n_tc_launches, int *n_cc_launches);
+
+/* ---- FP8-E4M3 forward (no counterpart in the reference, which computes in
+ * FP16 only; src/our_spmm.cu:109-145 uses FP16 mma.sync) ----
+ * A is quantized per sorted row, B per column: s = max|x| / 448 (1 for an
+ * all-zero row or column), q = E4M3(x / s) rounded to nearest even and
+ * saturated. The forward accumulates the exact products q_a * q_b in FP32 and
+ * returns alpha * (sum * s_a[row] * s_b[col]) + beta * C. */
+
+/* Builds (or, after new values, refreshes) the plan's E4M3 form of A.
+ * tca_spmm_fp8 calls it on first use; tca_plan_update_values refreshes it. */
+TCA_API int tca_plan_quantize_fp8(tca_plan_t plan, tca_stream_t stream);
+/* B (K x N FP16, row stride ldb) -> Bq (K x N E4M3 bytes, row stride ldq,
+ * ldq % 4 == 0) and scale[N] (FP32). */
+TCA_API int tca_quantize_b_fp8(const void *d_B_f16, int ldb, int K, int N, void *d_Bq, int ldq, float *d_scale,
+                               tca_stream_t stream);
+/* E4M3 forward from FP16 B, which is quantized per call into a workspace
+ * owned by the plan (allocated on first use, grown when N grows). Needs
+ * N % 8 == 0 and a 16-byte aligned C with ldc * sizeof(C) % 16 == 0. Calls
+ * on one plan must not overlap in time on different streams (they share the
+ * workspace). */
+TCA_API int tca_spmm_fp8(tca_plan_t plan, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype,
+                         float alpha, float beta, unsigned flags, tca_stream_t stream);
+/* tca_spmm_fp8 over many forwards in as few launches as tca_spmm_batched; a
+ * plan may appear once per batch. n_tile: 128 or 256 (0 = by N). */
+TCA_API int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
+                                 unsigned flags, tca_stream_t stream, void *const *events);
 
 /* ------------------------------------------------------------------ */
 /* Host-side matrix I/O and format conversion. Arrays returned through

@@ -61,6 +61,10 @@ def lib() -> ctypes.CDLL:
         L.orc_plan_build.argtypes = [_P, _P, _P, _I, _I, _I, _I, ctypes.c_float, _I, ctypes.POINTER(OrcPlan)]
         L.orc_plan_build.restype = _I
         L.orc_plan_free.argtypes = [ctypes.POINTER(OrcPlan)]; L.orc_plan_free.restype = None
+        L.orc_f32_to_e4m3.argtypes = [ctypes.c_float]; L.orc_f32_to_e4m3.restype = ctypes.c_uint8
+        L.orc_e4m3_to_f32.argtypes = [ctypes.c_uint8]; L.orc_e4m3_to_f32.restype = ctypes.c_float
+        L.orc_quant_rows.argtypes = [_I, _P, _P, _P, _P]; L.orc_quant_rows.restype = None
+        L.orc_quant_cols.argtypes = [_I, _I, _P, _I, _P, _I, _P]; L.orc_quant_cols.restype = None
         _lib = L
     return _lib
 
@@ -201,6 +205,57 @@ def build_plan(row_ptr, col_idx, vals, K, sort_rows=True, tc_min_density=0.02, p
 
 
 # ---------------------------------------------------------------- reference library
+def e4m3_table() -> np.ndarray:
+    """The FP32 value of every E4M3 code (orc_e4m3_to_f32); NaN codes are NaN."""
+    L = lib()
+    return np.array([L.orc_e4m3_to_f32(q) for q in range(256)], dtype=np.float32)
+
+
+def f32_to_e4m3(x) -> np.ndarray:
+    """Elementwise E4M3 encoding, round to nearest even, saturating (orc_f32_to_e4m3)."""
+    L = lib()
+    x = np.asarray(x, dtype=np.float32)
+    return np.array([L.orc_f32_to_e4m3(float(v)) for v in x.ravel()], dtype=np.uint8).reshape(x.shape)
+
+
+def quant_rows(row_ptr, vals):
+    """(scale[M] float32, q[nnz] uint8): per-row E4M3 quantization of CSR values (orc_quant_rows)."""
+    rp = _c(row_ptr, np.int32)
+    v = f16_bits(vals)
+    M = rp.size - 1
+    scale = np.empty(M, np.float32)
+    q = np.empty(v.size, np.uint8)
+    lib().orc_quant_rows(M, rp.ctypes.data, v.ctypes.data, scale.ctypes.data, q.ctypes.data)
+    return scale, q
+
+
+def quant_cols(B, ldq=None):
+    """(q[K, ldq] uint8, scale[N] float32): per-column E4M3 quantization of B (orc_quant_cols)."""
+    b = f16_bits(B)
+    K, N = b.shape
+    ldq = ldq or N
+    q = np.zeros((K, ldq), np.uint8)
+    scale = np.empty(N, np.float32)
+    lib().orc_quant_cols(K, N, b.ctypes.data, N, q.ctypes.data, ldq, scale.ctypes.data)
+    return q, scale
+
+
+def spmm_fp8_f64(row_ptr, col_idx, vals, B):
+    """FP64 product of the dequantized operands: (s_a[r] q_a) (s_b[n] q_b) summed in FP64 --
+    what the E4M3 forward computes, up to FP32 accumulation."""
+    tab = e4m3_table().astype(np.float64)
+    sa, qa = quant_rows(row_ptr, vals)
+    qb, sb = quant_cols(B)
+    import scipy.sparse as sp
+    rp = np.asarray(row_ptr)
+    M = rp.size - 1
+    rows = np.repeat(np.arange(M), np.diff(rp))
+    a = tab[qa] * sa.astype(np.float64)[rows]
+    b = tab[qb] * sb.astype(np.float64)[None, :]
+    A = sp.csr_matrix((a, np.asarray(col_idx), rp), shape=(M, b.shape[0]))
+    return np.asarray(A @ b)
+
+
 def ref_available() -> bool:
     return REF_PATH.exists()
 

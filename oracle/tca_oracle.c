@@ -546,3 +546,71 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
     free(cur); free(rank); free(is_tc); free(nch); free(wnnz); free(direct); free(row_nnz); free(row_sorted);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------
+ * FP8-E4M3 quantization (the rebuild's reduced-precision mode; the reference
+ * computes in FP16 only). E4M3: 1 sign, 4 exponent (bias 7), 3 mantissa bits,
+ * no infinities, 0x7F / 0xFF are NaN, largest finite 448, smallest subnormal
+ * 2^-9. Conversion: round to nearest, ties to even, saturating to +-448.
+ * ------------------------------------------------------------------------- */
+uint8_t orc_f32_to_e4m3(float x)
+{
+    if (isnan(x)) return 0x7F;
+    const uint8_t sign = signbit(x) ? 0x80 : 0x00;
+    const float a = fabsf(x);
+    if (a >= 448.0f) return sign | 0x7E; /* saturate (448 = 1.75 * 2^8) */
+    if (a < 0.015625f) {                  /* below 2^-6: subnormal, quantum 2^-9 */
+        const float m = nearbyintf(a * 512.0f); /* exact scaling; ties to even */
+        return sign | (uint8_t)m;          /* m == 8 is the smallest normal, 0x08 */
+    }
+    int e;
+    frexpf(a, &e);                        /* a = f * 2^e, f in [0.5, 1) */
+    int E = e - 1;                        /* a in [2^E, 2^(E+1)), E in [-6, 8] */
+    float m = nearbyintf(ldexpf(a, 3 - E)); /* 8 .. 16 */
+    if (m >= 16.0f) { m = 8.0f; E += 1; }
+    if (E > 8) return sign | 0x7E;
+    return sign | (uint8_t)(((E + 7) << 3) | ((int)m - 8));
+}
+
+float orc_e4m3_to_f32(uint8_t q)
+{
+    const float sign = (q & 0x80) ? -1.0f : 1.0f;
+    const int ex = (q >> 3) & 0xF, man = q & 7;
+    if ((q & 0x7F) == 0x7F) return NAN;
+    if (ex == 0) return sign * ldexpf((float)man, -9);
+    return sign * ldexpf(1.0f + man / 8.0f, ex - 7);
+}
+
+static float orc_scale_of(float amax) { return amax > 0.0f ? amax / 448.0f : 1.0f; }
+
+/* Per row r of a CSR (FP16 values): scale[r] = max|v| / 448 (1 if 0), q[j] =
+ * E4M3(v_j / scale[r]). */
+void orc_quant_rows(int M, const int *row_ptr, const uint16_t *val, float *scale, uint8_t *q)
+{
+    for (int r = 0; r < M; r++) {
+        float m = 0.0f;
+        for (int j = row_ptr[r]; j < row_ptr[r + 1]; j++) {
+            const float a = fabsf(orc_h2f(val[j]));
+            if (a > m) m = a;
+        }
+        const float s = orc_scale_of(m);
+        scale[r] = s;
+        for (int j = row_ptr[r]; j < row_ptr[r + 1]; j++) q[j] = orc_f32_to_e4m3(orc_h2f(val[j]) / s);
+    }
+}
+
+/* Per column n of B (K x N FP16, row stride ldb): scale[n] = max_k |B| / 448,
+ * q[k * ldq + n] = E4M3(B[k, n] / scale[n]). */
+void orc_quant_cols(int K, int N, const uint16_t *B, int ldb, uint8_t *q, int ldq, float *scale)
+{
+    for (int n = 0; n < N; n++) {
+        float m = 0.0f;
+        for (int k = 0; k < K; k++) {
+            const float a = fabsf(orc_h2f(B[(size_t)k * ldb + n]));
+            if (a > m) m = a;
+        }
+        scale[n] = orc_scale_of(m);
+    }
+    for (int k = 0; k < K; k++)
+        for (int n = 0; n < N; n++) q[(size_t)k * ldq + n] = orc_f32_to_e4m3(orc_h2f(B[(size_t)k * ldb + n]) / scale[n]);
+}

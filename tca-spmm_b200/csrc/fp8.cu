@@ -1,0 +1,318 @@
+// fp8.cu -- the FP8-E4M3 forward: quantization of A (per sorted row) and of
+// B (per column), and the entry points that run the tensor-core and CUDA-core
+// kernels on the quantized operands.
+//
+// Scales: s = max|x| / 448 over the row of A (or column of B); 1 when the row
+// or column is all zero. Values: q = E4M3(x / s), round to nearest even,
+// saturating at +-448 (cvt.rn.satfinite). Products q_a * q_b are exact in
+// FP32; sums accumulate in FP32; the result is multiplied by s_a[row] *
+// s_b[col] before alpha / beta.
+//
+// The reference has no reduced-precision path; this is a new component of the
+// rebuild, checked against a CPU restatement of the same quantization.
+#include <cuda_fp8.h>
+#include <algorithm>
+#include <vector>
+#include "tca_internal.cuh"
+#include "plan.cuh"
+
+namespace tca {
+namespace {
+
+__device__ __forceinline__ uint8_t to_e4m3(float x)
+{
+    return (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
+}
+
+__device__ __forceinline__ float scale_of(float amax) { return amax > 0.f ? amax / kE4M3Max : 1.f; }
+
+// One warp per sorted row: the row's scale and its quantized values.
+__global__ void k_quant_rows(const int *__restrict__ p_row_ptr, const __half *__restrict__ p_val, int M,
+                             float *__restrict__ row_scale, uint8_t *__restrict__ p_val_f8)
+{
+    const int lane = threadIdx.x & 31;
+    const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= M)
+        return;
+    const int j0 = p_row_ptr[r], j1 = p_row_ptr[r + 1];
+    float m = 0.f;
+    for (int j = j0 + lane; j < j1; j += 32) m = fmaxf(m, fabsf(__half2float(p_val[j])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const float s = scale_of(m);
+    if (lane == 0)
+        row_scale[r] = s;
+    for (int j = j0 + lane; j < j1; j += 32) p_val_f8[j] = to_e4m3(__half2float(p_val[j]) / s);
+}
+
+// Tile entries with their E4M3 value in the low byte (tile_src indexes p_val).
+__global__ void k_entries_f8(const uint32_t *__restrict__ entries, const int *__restrict__ tile_src,
+                             const uint8_t *__restrict__ p_val_f8, uint32_t *__restrict__ out, long long n)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = (entries[i] & 0xffff0000u) | (uint32_t)p_val_f8[tile_src[i]];
+}
+
+// Dense 128 x 64 E4M3 images in the 64-byte swizzled K-major layout.
+__global__ void __launch_bounds__(256)
+k_render_images_f8(const int *__restrict__ img_chunk, const int *__restrict__ tile_ptr,
+                   const uint32_t *__restrict__ entries_f8, uint8_t *__restrict__ images)
+{
+    const int m = blockIdx.x;
+    const int c = img_chunk[m];
+    uint8_t *img = images + (size_t)m * kWindowRows * kChunkCols;
+    for (int k = threadIdx.x; k < kWindowRows * kChunkCols / 16; k += blockDim.x)
+        reinterpret_cast<uint4 *>(img)[k] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    for (int e = tile_ptr[c] + threadIdx.x; e < tile_ptr[c + 1]; e += blockDim.x) {
+        const uint32_t v = entries_f8[e];
+        img[swz64_offset(v >> 22, (v >> 16) & 63u)] = (uint8_t)(v & 0xffu);
+    }
+}
+
+// Column absolute maxima of B (as FP32 bit patterns, which order like the
+// non-negative values): thread = column, block row = 32 rows of B.
+__global__ void k_col_absmax(const __half *__restrict__ B, int ldb, int K, int N, unsigned *__restrict__ colmax)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N)
+        return;
+    const int k0 = blockIdx.y * 32, k1 = min(K, k0 + 32);
+    float m = 0.f;
+    for (int k = k0; k < k1; k++) m = fmaxf(m, fabsf(__half2float(B[(size_t)k * ldb + n])));
+    atomicMax(colmax + n, __float_as_uint(m));
+}
+
+// Bq[k, n] = E4M3(B[k, n] / s[n]); thread = 4 consecutive columns of one row.
+__global__ void k_quant_cols(const __half *__restrict__ B, int ldb, int K, int N, const unsigned *__restrict__ colmax,
+                             uint8_t *__restrict__ Bq, int ldq)
+{
+    const int n = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    if (n >= N)
+        return;
+    float s[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) s[i] = n + i < N ? scale_of(__uint_as_float(colmax[n + i])) : 1.f;
+    for (int k = blockIdx.y; k < K; k += gridDim.y) {
+        uint32_t packed = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            if (n + i < N)
+                packed |= (uint32_t)to_e4m3(__half2float(B[(size_t)k * ldb + n + i]) / s[i]) << (8 * i);
+        if (n + 4 <= N) {
+            *reinterpret_cast<uint32_t *>(Bq + (size_t)k * ldq + n) = packed;
+        } else {
+            for (int i = 0; n + i < N; i++) Bq[(size_t)k * ldq + n + i] = (uint8_t)(packed >> (8 * i));
+        }
+    }
+}
+
+// colmax (bit patterns) -> scales, in place.
+__global__ void k_col_scale(unsigned *__restrict__ colmax, int N)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n < N) {
+        const float s = scale_of(__uint_as_float(colmax[n]));
+        colmax[n] = __float_as_uint(s);
+    }
+}
+
+unsigned blocks(long long n, int per) { return (unsigned)((n + per - 1) / per); }
+
+int quantize_b(const __half *B, int ldb, int K, int N, uint8_t *Bq, int ldq, float *scale, cudaStream_t s)
+{
+    if (K <= 0 || N <= 0)
+        return TCA_OK;
+    unsigned *colmax = reinterpret_cast<unsigned *>(scale);
+    TCA_CUDA_TRY(cudaMemsetAsync(colmax, 0, sizeof(unsigned) * (size_t)N, s));
+    k_col_absmax<<<dim3(blocks(N, 256), blocks(K, 32)), 256, 0, s>>>(B, ldb, K, N, colmax);
+    k_quant_cols<<<dim3(blocks(blocks(N, 4), 128), (unsigned)std::min(K, 65535)), 128, 0, s>>>(B, ldb, K, N, colmax, Bq, ldq);
+    k_col_scale<<<blocks(N, 256), 256, 0, s>>>(colmax, N);
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
+int quantize_plan(tca_plan *p, cudaStream_t s)
+{
+    if (!p->row_scale) {
+        auto alloc = [&](void **ptr, size_t b) -> int {
+            const cudaError_t e = cudaMalloc(ptr, b > 0 ? b : 16);
+            if (e != cudaSuccess)
+                return set_error(TCA_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+            p->bytes += b;
+            return TCA_OK;
+        };
+        TCA_TRY(alloc((void **)&p->row_scale, sizeof(float) * (size_t)p->M));
+        TCA_TRY(alloc((void **)&p->p_val_f8, (size_t)p->nnz));
+        TCA_TRY(alloc((void **)&p->tile_entries_f8, sizeof(uint32_t) * ((size_t)p->tc_nnz + kEntryPad)));
+        TCA_TRY(alloc((void **)&p->images_f8, (size_t)p->n_images * kWindowRows * kChunkCols));
+        TCA_CUDA_TRY(cudaMemsetAsync(p->tile_entries_f8, 0, sizeof(uint32_t) * ((size_t)p->tc_nnz + kEntryPad), s));
+    }
+    if (p->M > 0)
+        k_quant_rows<<<blocks((long long)p->M * 32, 256), 256, 0, s>>>(p->p_row_ptr, p->p_val, p->M, p->row_scale,
+                                                                       p->p_val_f8);
+    if (p->tc_nnz > 0)
+        k_entries_f8<<<blocks(p->tc_nnz, 256), 256, 0, s>>>(p->tile_entries, p->tile_src, p->p_val_f8,
+                                                            p->tile_entries_f8, p->tc_nnz);
+    if (p->n_images > 0)
+        k_render_images_f8<<<p->n_images, 256, 0, s>>>(p->img_chunk, p->tile_ptr, p->tile_entries_f8, p->images_f8);
+    TCA_CUDA_TRY(cudaGetLastError());
+    p->has_fp8 = true;
+    return TCA_OK;
+}
+
+// The plan's B workspace for E4M3 forwards: K x ldq bytes, then N scales.
+int plan_workspace(tca_plan *p, int N, uint8_t **Bq, int *ldq, float **scale)
+{
+    const int q = (N + 15) & ~15;
+    const size_t bq = ((size_t)p->K * q + 255) & ~(size_t)255;
+    const size_t need = bq + sizeof(float) * (size_t)q;
+    if (need > p->fp8_ws_bytes) {
+        if (p->fp8_ws) {
+            cudaFree(p->fp8_ws); // synchronises with work that still reads it
+            p->bytes -= p->fp8_ws_bytes;
+            p->fp8_ws = nullptr;
+            p->fp8_ws_bytes = 0;
+        }
+        const cudaError_t e = cudaMalloc(&p->fp8_ws, need);
+        if (e != cudaSuccess)
+            return set_error(TCA_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", need, cudaGetErrorString(e));
+        p->fp8_ws_bytes = need;
+        p->bytes += need;
+    }
+    *Bq = static_cast<uint8_t *>(p->fp8_ws);
+    *ldq = q;
+    *scale = reinterpret_cast<float *>(static_cast<uint8_t *>(p->fp8_ws) + bq);
+    return TCA_OK;
+}
+
+int make_fp8_job(tca_plan_t p, const void *B, int ldb, int N, void *C, int ldc, int c_dtype, bool batched,
+                 cudaStream_t s, SpmmJob *job)
+{
+    if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    TCA_TRY(check_dense_args(B, ldb, N, C, ldc, c_dtype, p->M, p->K));
+    const size_t c_elem = c_dtype == TCA_DTYPE_F16 ? 2 : 4;
+    if (p->M > 0 && N > 0 && (N % 8 != 0 || !aligned16(C) || ((size_t)ldc * c_elem) % 16 != 0))
+        return set_error(TCA_ERR_UNSUPPORTED,
+                         "the E4M3 forward needs N %% 8 == 0 and a 16-byte aligned C with 16-byte aligned rows");
+    if (!p->has_fp8)
+        TCA_TRY(quantize_plan(p, s));
+    job->p = p;
+    job->B = (const __half *)B;
+    job->C = C;
+    job->ldb = ldb;
+    job->N = N;
+    job->ldc = ldc;
+    job->f8 = true;
+    job->tc = p->n_tc > 0;
+    job->n_tile = pick_tc_tile(p->n_tc, N, batched, true);
+    if (p->M == 0 || N == 0 || p->K == 0)
+        return TCA_OK;
+    uint8_t *Bq;
+    float *scale;
+    int ldq;
+    TCA_TRY(plan_workspace(p, N, &Bq, &ldq, &scale));
+    TCA_TRY(quantize_b((const __half *)B, ldb, p->K, N, Bq, ldq, scale, s));
+    job->Bq = Bq;
+    job->ldq = ldq;
+    job->col_scale = scale;
+    return TCA_OK;
+}
+
+} // namespace
+
+int plan_requantize_fp8(tca_plan *p, cudaStream_t s)
+{
+    return p->has_fp8 ? quantize_plan(p, s) : TCA_OK;
+}
+
+void plan_free_fp8(tca_plan *p)
+{
+    void *arrs[] = {p->row_scale, p->p_val_f8, p->tile_entries_f8, p->images_f8, p->fp8_ws};
+    for (void *a : arrs)
+        if (a) cudaFree(a);
+    p->row_scale = nullptr;
+    p->p_val_f8 = nullptr;
+    p->tile_entries_f8 = nullptr;
+    p->images_f8 = nullptr;
+    p->fp8_ws = nullptr;
+    p->fp8_ws_bytes = 0;
+    p->has_fp8 = false;
+}
+
+} // namespace tca
+
+using namespace tca;
+
+int tca_plan_quantize_fp8(tca_plan_t p, tca_stream_t stream)
+{
+    clear_error();
+    if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    return quantize_plan(p, (cudaStream_t)stream);
+}
+
+int tca_quantize_b_fp8(const void *d_B_f16, int ldb, int K, int N, void *d_Bq, int ldq, float *d_scale,
+                       tca_stream_t stream)
+{
+    clear_error();
+    if (K < 0 || N < 0) return set_error(TCA_ERR_INVALID_ARG, "negative size (K=%d, N=%d)", K, N);
+    if (K == 0 || N == 0) return TCA_OK;
+    if (!d_B_f16 || !d_Bq || !d_scale) return set_error(TCA_ERR_INVALID_ARG, "NULL buffer");
+    if (ldb < N || ldq < N) return set_error(TCA_ERR_INVALID_ARG, "ldb (%d) and ldq (%d) must be >= N (%d)", ldb, ldq, N);
+    if (ldq % 4 != 0 || (reinterpret_cast<uintptr_t>(d_Bq) & 3u) || (reinterpret_cast<uintptr_t>(d_scale) & 3u))
+        return set_error(TCA_ERR_INVALID_ARG, "Bq needs 4-byte aligned rows (ldq %% 4 == 0) and scale 4-byte alignment");
+    return quantize_b((const __half *)d_B_f16, ldb, K, N, (uint8_t *)d_Bq, ldq, d_scale, (cudaStream_t)stream);
+}
+
+int tca_spmm_fp8(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype, float alpha,
+                 float beta, unsigned flags, tca_stream_t stream)
+{
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    SpmmJob job;
+    TCA_TRY(make_fp8_job(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, false, s, &job));
+    if (p->M == 0 || N == 0) return TCA_OK;
+    if (p->K == 0) // no nonzeros can exist: A B = 0
+        return tca_spmm(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, alpha, beta, flags, stream);
+    TCA_TRY(launch_tc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
+    TCA_TRY(launch_cc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
+    return TCA_OK;
+}
+
+int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
+                         unsigned flags, tca_stream_t stream, void *const *events)
+{
+    clear_error();
+    if (n_items < 0 || (n_items > 0 && !items))
+        return set_error(TCA_ERR_INVALID_ARG, "invalid batch");
+    cudaStream_t s = (cudaStream_t)stream;
+    std::vector<SpmmJob> jobs;
+    jobs.reserve((size_t)n_items);
+    for (int i = 0; i < n_items; i++) {
+        const tca_batch_item_t &it = items[i];
+        for (int k = 0; k < i; k++)
+            if (items[k].plan == it.plan)
+                return set_error(TCA_ERR_INVALID_ARG,
+                                 "batch items %d and %d share a plan: an E4M3 batch quantizes B into the plan", k, i);
+        SpmmJob j;
+        TCA_TRY(make_fp8_job(it.plan, it.d_B_f16, it.ldb, it.N, it.d_C, it.ldc, c_dtype, true, s, &j));
+        if (it.n_tile == 128 || it.n_tile == 256)
+            j.n_tile = it.n_tile;
+        if (it.plan->M > 0 && it.N > 0 && it.plan->K == 0) // no nonzeros can exist: A B = 0
+            TCA_TRY(tca_spmm(it.plan, it.d_B_f16, it.ldb, it.N, it.d_C, it.ldc, c_dtype, alpha, beta, flags, stream));
+        else if (it.plan->M > 0 && it.N > 0)
+            jobs.push_back(j);
+    }
+    auto rec = [&](int i) -> int {
+        if (events && events[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[i], s));
+        return TCA_OK;
+    };
+    TCA_TRY(rec(0));
+    TCA_TRY(launch_tc_jobs(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s));
+    TCA_TRY(rec(1));
+    TCA_TRY(rec(2));
+    TCA_TRY(launch_cc_jobs(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s));
+    TCA_TRY(rec(3));
+    return TCA_OK;
+}

@@ -301,6 +301,7 @@ void free_plan(tca_plan *p)
 {
     if (!p) return;
     transpose_free(p);
+    plan_free_fp8(p);
     void *arrs[] = {p->perm, p->p_row_ptr, p->p_col, p->p_val, p->src, p->tc_windows, p->cc_windows,
                     p->all_windows, p->tile_first, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src,
                     p->img_idx, p->images, p->img_chunk, p->cc_items, p->all_items, p->tc_win_info,
@@ -599,6 +600,7 @@ int tca_plan_update_values(tca_plan_t p, const void *d_vals_f16, tca_stream_t st
     if (p->n_images > 0)
         k_render_images<<<p->n_images, 256, 0, s>>>(p->img_chunk, p->tile_ptr, p->tile_entries, p->images);
     TCA_CUDA_TRY(cudaGetLastError());
+    TCA_TRY(plan_requantize_fp8(p, s));
     return transpose_update_values(p, (const __half *)d_vals_f16, s);
 }
 
@@ -641,6 +643,13 @@ int tca_plan_export(tca_plan_t p, int which, void *h_dst, size_t capacity, size_
     case TCA_ARR_TILE_IMAGES: src = p->images; n = sizeof(uint16_t) * (size_t)p->n_images * kWindowRows * kChunkCols; break;
     case TCA_ARR_CC_ITEMS: src = p->cc_items; n = sizeof(int2) * (size_t)p->n_cc_items; break;
     case TCA_ARR_ALL_ITEMS: src = p->all_items; n = sizeof(int2) * (size_t)p->n_all_items; break;
+    case TCA_ARR_ROW_SCALE: src = p->row_scale; n = p->has_fp8 ? sizeof(float) * (size_t)p->M : 0; break;
+    case TCA_ARR_P_VAL_F8: src = p->p_val_f8; n = p->has_fp8 ? (size_t)p->nnz : 0; break;
+    case TCA_ARR_TILE_ENTRIES_F8: src = p->tile_entries_f8; n = p->has_fp8 ? sizeof(uint32_t) * (size_t)p->tc_nnz : 0; break;
+    case TCA_ARR_TILE_IMAGES_F8:
+        src = p->images_f8;
+        n = p->has_fp8 ? (size_t)p->n_images * kWindowRows * kChunkCols : 0;
+        break;
     default: return set_error(TCA_ERR_INVALID_ARG, "unknown plan array %d", which);
     }
     if (out_bytes) *out_bytes = n;

@@ -118,7 +118,13 @@ struct SpmmJob {
     void *C;
     int ldb, N, ldc;
     bool tc;    // the plan's tensor-core windows run on tensor cores
-    int n_tile; // tensor-core N-slice width (64, 128, 256)
+    int n_tile; // tensor-core N-slice width (64, 128, 256; 128 or 256 for E4M3)
+    // E4M3 forward: B quantized per column (K x N bytes, row stride ldq) with
+    // its column scales; A's E4M3 form lives in the plan.
+    bool f8 = false;
+    const uint8_t *Bq = nullptr;
+    int ldq = 0;
+    const float *col_scale = nullptr;
 };
 
 // Tensor-core (tcgen05) forward over the tensor-core windows of every job
@@ -132,7 +138,11 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
                    cudaStream_t s);
 
 // The N-slice width a single forward of this plan uses.
-int pick_tc_tile(int n_tc, int N, bool batched);
+int pick_tc_tile(int n_tc, int N, bool batched, bool f8 = false);
+
+// E4M3 form of A (fp8.cu): refresh after new values (when it exists); release.
+int plan_requantize_fp8(tca_plan *p, cudaStream_t s);
+void plan_free_fp8(tca_plan *p);
 
 // The plan of A^T (adjoint.cu): propagate new caller-order values; release.
 int transpose_update_values(tca_plan *p, const __half *vals, cudaStream_t s);

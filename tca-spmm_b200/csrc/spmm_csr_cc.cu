@@ -19,6 +19,7 @@
 // nonzeros whose column is outside [0, K) contribute nothing.
 #include <algorithm>
 #include <vector>
+#include <cuda_fp8.h>
 #include "tca_internal.cuh"
 #include "plan.cuh"
 #include "ptx.cuh"
@@ -240,6 +241,10 @@ struct CcJob {
     const __half *p_val;
     const __half *B;
     void *C;
+    // E4M3 forward: values, B (row stride ldq bytes) and their scales
+    const uint8_t *p_val8, *Bq;
+    const float *row_scale, *col_scale;
+    int ldq;
     int n_items;
     int M, K, N, ldb, ldc;
     float alpha, beta;
@@ -429,28 +434,48 @@ __device__ __forceinline__ ItemDesc load_desc(const CcBatch &b, int item)
     return d;
 }
 
-template <typename OutT, int W>
+// B vectors of W elements: W halves, or W E4M3 bytes.
+template <int W, bool F8> struct BVec { using T = typename HalfVec<W>::T; };
+template <> struct BVec<8, true> { using T = uint2; };
+template <> struct BVec<4, true> { using T = unsigned; };
+template <> struct BVec<2, true> { using T = unsigned short; };
+
+// F8: values and B are E4M3 (every E4M3 value is an FP16 value, so the
+// products are formed exactly by the same mixed-precision FMA); the flush
+// multiplies the FP32 sum by row scale x column scale, as the tensor-core
+// epilogue does.
+template <typename OutT, int W, bool F8>
 __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(const __grid_constant__ CcBatch b)
 {
-    using V = typename HalfVec<W>::T;
+    using V = typename BVec<W, F8>::T;
     constexpr int U = 8;
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int n_warps = (int)gridDim.x * 8;
     int item = (int)blockIdx.x * 8 + (int)(threadIdx.x >> 5);
 
-    // row offsets (lane k <= nrows) and output rows (lane k < nrows) of an item
-    auto load_rows = [&](const ItemDesc &d, int &rs, int &orow) {
+    // row offsets (lane k <= nrows), output rows and E4M3 row scales (lane k < nrows) of an item
+    auto load_rows = [&](const ItemDesc &d, int &rs, int &orow, float &sc) {
         rs = 0;
         orow = 0;
+        sc = 0.f;
         if (lane <= d.nrows && d.nrows > 0) {
             const CcJob &a = b.job[d.job];
             rs = __ldg(a.p_row_ptr + d.r0 + lane);
-            if (lane < d.nrows)
+            if (lane < d.nrows) {
                 orow = __ldg(a.perm + d.r0 + lane);
+                if constexpr (F8)
+                    sc = __ldg(a.row_scale + d.r0 + lane);
+            }
         }
     };
-    // the item's first 32 nonzeros, one per lane
+    auto value = [&](const CcJob &a, int j) -> unsigned short {
+        if constexpr (F8)
+            return __nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)a.p_val8[j], __NV_E4M3).x;
+        else
+            return __half_as_ushort(a.p_val[j]);
+    };
+    // the item's first 32 nonzeros, one per lane (values as FP16 bits)
     auto load_nz = [&](const ItemDesc &d, int rs, int &col, unsigned short &val) {
         const int j0 = __shfl_sync(full, rs, 0), j1 = __shfl_sync(full, rs, d.nrows & 31);
         col = 0;
@@ -458,15 +483,16 @@ __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(con
         if (d.nrows > 0 && j0 + lane < j1) {
             const CcJob &a = b.job[d.job];
             col = __ldg(a.p_col + j0 + lane);
-            val = __half_as_ushort(a.p_val[j0 + lane]);
+            val = value(a, j0 + lane);
         }
     };
 
     ItemDesc d0 = load_desc(b, item), d1 = load_desc(b, item + n_warps), d2 = load_desc(b, item + 2 * n_warps);
     int rs0, out0, rs1, out1, col0;
+    float sc0, sc1;
     unsigned short val0;
-    load_rows(d0, rs0, out0);
-    load_rows(d1, rs1, out1);
+    load_rows(d0, rs0, out0, sc0);
+    load_rows(d1, rs1, out1, sc1);
     load_nz(d0, rs0, col0, val0);
 
     while (d0.nrows > 0) {
@@ -475,7 +501,8 @@ __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(con
         unsigned short val1;
         load_nz(d1, rs1, col1, val1);
         int rs2, out2;
-        load_rows(d2, rs2, out2);
+        float sc2;
+        load_rows(d2, rs2, out2, sc2);
         const ItemDesc d3 = load_desc(b, item + 3 * n_warps);
 
         // ---- item i
@@ -486,7 +513,14 @@ __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(con
         for (int nb = 0; nb < a.N; nb += 32 * W) {
             const int n0 = nb + lane * W;
             const bool active = n0 < a.N;
-            const __half *Bn = a.B + (active ? n0 : 0);
+            const uint8_t *Bn = F8 ? a.Bq + (active ? n0 : 0)
+                                   : reinterpret_cast<const uint8_t *>(a.B + (active ? n0 : 0));
+            const size_t brow = F8 ? (size_t)a.ldq : (size_t)a.ldb * 2; // bytes per B row
+            float sb[F8 ? W : 1];
+            if constexpr (F8) {
+#pragma unroll
+                for (int i = 0; i < W; i++) sb[i] = active ? __ldg(a.col_scale + n0 + i) : 0.f;
+            }
             float acc[W];
 #pragma unroll
             for (int i = 0; i < W; i++) acc[i] = 0.f;
@@ -495,17 +529,27 @@ __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(con
             auto flush = [&]() {
                 const int rstart = __shfl_sync(full, rs0, cr);
                 const int orow = __shfl_sync(full, out0, cr);
+                float sa = 1.f;
+                if constexpr (F8)
+                    sa = __shfl_sync(full, sc0, cr);
                 if (active && !(keep && rstart == ce)) {
                     OutT *cp = reinterpret_cast<OutT *>(a.C) + (size_t)orow * a.ldc + n0;
-                    float o[W];
+                    float t[W], o[W];
+#pragma unroll
+                    for (int i = 0; i < W; i++) {
+                        if constexpr (F8)
+                            t[i] = acc[i] * (sa * sb[i]);
+                        else
+                            t[i] = acc[i];
+                    }
                     if (a.beta != 0.f) {
                         float old[W];
                         load_out<W>(cp, old);
 #pragma unroll
-                        for (int i = 0; i < W; i++) o[i] = fmaf(a.alpha, acc[i], a.beta * old[i]);
+                        for (int i = 0; i < W; i++) o[i] = fmaf(a.alpha, t[i], a.beta * old[i]);
                     } else {
 #pragma unroll
-                        for (int i = 0; i < W; i++) o[i] = a.alpha * acc[i];
+                        for (int i = 0; i < W; i++) o[i] = a.alpha * t[i];
                     }
                     store_out<W>(cp, o);
                 }
@@ -523,7 +567,7 @@ __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(con
                     v = 0;
                     if (base + lane < j1) {
                         c = __ldg(a.p_col + base + lane);
-                        v = __half_as_ushort(a.p_val[base + lane]);
+                        v = value(a, base + lane);
                     }
                 }
                 const int m = min(32, j1 - base);
@@ -536,15 +580,25 @@ __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(con
                         av[u] = (unsigned short)__shfl_sync(full, (int)v, t + u);
                         bv[u] = V{};
                         if (active && t + u < m)
-                            bv[u] = __ldg(reinterpret_cast<const V *>(Bn + (size_t)cu * a.ldb));
+                            bv[u] = __ldg(reinterpret_cast<const V *>(Bn + (size_t)cu * brow));
                     }
 #pragma unroll
                     for (int u = 0; u < U; u++) {
                         if (t + u < m) { // uniform across the warp
                             while (base + t + u >= ce) flush();
-                            const unsigned short *h = reinterpret_cast<const unsigned short *>(&bv[u]);
+                            if constexpr (F8) {
+                                const __nv_fp8x2_storage_t *q = reinterpret_cast<const __nv_fp8x2_storage_t *>(&bv[u]);
 #pragma unroll
-                            for (int i = 0; i < W; i++) acc[i] = fma_f16_f32(av[u], h[i], acc[i]);
+                                for (int i = 0; i < W / 2; i++) {
+                                    const __half2_raw h = __nv_cvt_fp8x2_to_halfraw2(q[i], __NV_E4M3);
+                                    acc[2 * i] = fma_f16_f32(av[u], h.x, acc[2 * i]);
+                                    acc[2 * i + 1] = fma_f16_f32(av[u], h.y, acc[2 * i + 1]);
+                                }
+                            } else {
+                                const unsigned short *h = reinterpret_cast<const unsigned short *>(&bv[u]);
+#pragma unroll
+                                for (int i = 0; i < W; i++) acc[i] = fma_f16_f32(av[u], h[i], acc[i]);
+                            }
                         }
                     }
                 }
@@ -553,8 +607,8 @@ __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(con
         }
 
         // ---- rotate the pipeline
-        d0 = d1; rs0 = rs1; out0 = out1; col0 = col1; val0 = val1;
-        d1 = d2; rs1 = rs2; out1 = out2;
+        d0 = d1; rs0 = rs1; out0 = out1; sc0 = sc1; col0 = col1; val0 = val1;
+        d1 = d2; rs1 = rs2; out1 = out2; sc1 = sc2;
         d2 = d3;
         item += n_warps;
     }
@@ -632,7 +686,7 @@ int launch_cc_group(const CcBatch &b, cudaStream_t s)
 
 // Persistent grid of the stream kernel: enough warps for every item, at most
 // the resident blocks of all SMs.
-template <typename OutT, int W>
+template <typename OutT, int W, bool F8>
 int launch_stream_group(const CcBatch &b, cudaStream_t s)
 {
     const int total = b.item_start[b.n_jobs];
@@ -641,11 +695,11 @@ int launch_stream_group(const CcBatch &b, cudaStream_t s)
     static int per_sm = 0;
     if (per_sm == 0) {
         int n = 0;
-        TCA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spmm_cc_stream_kernel<OutT, W>, 256, 0));
+        TCA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spmm_cc_stream_kernel<OutT, W, F8>, 256, 0));
         per_sm = n > 0 ? n : 1;
     }
     const int grid = std::min((total + 7) / 8, kSMs * per_sm);
-    spmm_cc_stream_kernel<OutT, W><<<grid, 256, 0, s>>>(b);
+    spmm_cc_stream_kernel<OutT, W, F8><<<grid, 256, 0, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
 }
@@ -653,15 +707,21 @@ int launch_stream_group(const CcBatch &b, cudaStream_t s)
 // Columns per lane of the stream kernel: 8 for N > 128, 4 for N > 64, else 2.
 inline int pick_w(int N) { return N > 128 ? 8 : N > 64 ? 4 : 2; }
 
+template <typename OutT, bool F8>
+int launch_stream_w(const CcBatch &b, int w, cudaStream_t s)
+{
+    switch (w) {
+    case 2: return launch_stream_group<OutT, 2, F8>(b, s);
+    case 4: return launch_stream_group<OutT, 4, F8>(b, s);
+    default: return launch_stream_group<OutT, 8, F8>(b, s);
+    }
+}
+
 template <typename OutT>
-int launch_cc_typed(const CcBatch &b, int w, bool vec, cudaStream_t s)
+int launch_cc_typed(const CcBatch &b, int w, bool vec, bool f8, cudaStream_t s)
 {
     if (!vec) return launch_cc_group<OutT, 32, false>(b, s);
-    switch (w) {
-    case 2: return launch_stream_group<OutT, 2>(b, s);
-    case 4: return launch_stream_group<OutT, 4>(b, s);
-    default: return launch_stream_group<OutT, 8>(b, s);
-    }
+    return f8 ? launch_stream_w<OutT, true>(b, w, s) : launch_stream_w<OutT, false>(b, w, s);
 }
 
 } // namespace
@@ -669,16 +729,16 @@ int launch_cc_typed(const CcBatch &b, int w, bool vec, cudaStream_t s)
 int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
                    cudaStream_t s)
 {
-    // groups: (columns per lane, vectorised) -- stream kernel with 2/4/8 columns, plus scalar items
-    const int kinds[4][2] = {{2, 1}, {4, 1}, {8, 1}, {32, 0}};
+    // groups: (columns per lane, vectorised, E4M3) -- stream kernel with 2/4/8 columns, scalar items
+    const int kinds[7][3] = {{2, 1, 0}, {4, 1, 0}, {8, 1, 0}, {32, 0, 0}, {2, 1, 1}, {4, 1, 1}, {8, 1, 1}};
     for (const auto &kd : kinds) {
         CcBatch b;
         b.n_jobs = 0;
         b.block_start[0] = 0;
         b.item_start[0] = 0;
         auto flush = [&]() -> int {
-            const int st = (c_dtype == TCA_DTYPE_F16) ? launch_cc_typed<__half>(b, kd[0], kd[1] != 0, s)
-                                                      : launch_cc_typed<float>(b, kd[0], kd[1] != 0, s);
+            const int st = (c_dtype == TCA_DTYPE_F16) ? launch_cc_typed<__half>(b, kd[0], kd[1] != 0, kd[2] != 0, s)
+                                                      : launch_cc_typed<float>(b, kd[0], kd[1] != 0, kd[2] != 0, s);
             b.n_jobs = 0;
             return st;
         };
@@ -688,9 +748,10 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
             const int n_items = sj.tc ? p->n_cc_items : p->n_all_items;
             if (n_items == 0 || sj.N <= 0)
                 continue;
-            const bool vec = vec_ok(sj.B, sj.ldb, sj.N, sj.C, sj.ldc, c_dtype);
+            // E4M3 jobs always qualify (B is the library's own aligned copy; C was checked)
+            const bool vec = sj.f8 || vec_ok(sj.B, sj.ldb, sj.N, sj.C, sj.ldc, c_dtype);
             const int lpr = vec ? pick_w(sj.N) : 32;
-            if (lpr != kd[0] || (vec ? 1 : 0) != kd[1])
+            if (lpr != kd[0] || (vec ? 1 : 0) != kd[1] || (sj.f8 ? 1 : 0) != kd[2])
                 continue;
             CcJob &a = b.job[b.n_jobs];
             a.items = sj.tc ? p->cc_items : p->all_items;
@@ -700,6 +761,11 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
             a.p_val = p->p_val;
             a.B = sj.B;
             a.C = sj.C;
+            a.p_val8 = p->p_val_f8;
+            a.Bq = sj.Bq;
+            a.row_scale = p->row_scale;
+            a.col_scale = sj.col_scale;
+            a.ldq = sj.ldq;
             a.n_items = n_items;
             a.M = p->M;
             a.K = p->K;

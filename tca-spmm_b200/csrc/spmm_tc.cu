@@ -52,7 +52,6 @@ constexpr int kLoaderWarp1 = 10;     // warps 10..: TMA issue, chunks g = 1, 2, 
 constexpr int kLoaders = 4;          // loader warps, each issuing every kLoaders-th chunk
 constexpr int kThreads = 320 + (kLoaders - 1) * 32;
 constexpr int kMaxCtaItems = 32;      // work items per persistent CTA
-constexpr int kATileBytes = kWindowRows * kChunkCols * 2;     // 16 KB
 constexpr int kStagingBytes = ((kImageMinNnz + 3) * 4 + 15) & ~15; // entries of a sparse chunk, 16-byte rounded
 constexpr int kMaxJobs = 32;                                  // jobs per launch (kernel parameter space)
 
@@ -62,7 +61,9 @@ struct TcJob {
     const int4 *win_info; // per tensor-core window: window, first chunk, chunk count
     const int *tile_ptr, *win_cols, *img_idx, *perm, *p_row_ptr;
     const uint32_t *entries;
-    const uint16_t *images;
+    const uint8_t *images;   // dense tile images (16 KB FP16 or 8 KB E4M3 each)
+    const float *row_scale;  // E4M3: per sorted row
+    const float *col_scale;  // E4M3: per column of N
     const __half *B;
     void *C;
     int *status;
@@ -91,6 +92,14 @@ __device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b
     asm volatile("{\n\t.reg .pred p;\n\t"
                  "setp.ne.b32 p, %4, 0;\n\t"
                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+                 "l"(a), "l"(b), "r"(idesc), "r"(accum)
+                 : "memory");
+}
+__device__ __forceinline__ void umma_f8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
                  "l"(a), "l"(b), "r"(idesc), "r"(accum)
                  : "memory");
 }
@@ -131,9 +140,14 @@ __device__ __forceinline__ void store8_out(float *p, const float *v, float alpha
 // Shared memory (1024-byte aligned base): kStages x (A tile | B tile),
 // kStages entry staging buffers, per-stage chunk records, the CTA's item
 // table, mbarriers and two broadcast flags + TMEM slot.
-template <int NT> struct TcCfg {
-    static constexpr int kStages = NT == 256 ? 4 : NT == 128 ? 5 : 6;
-    static constexpr int kBTileBytes = kChunkCols * NT * 2;
+// F8: E4M3 operands -- an 8 KB A tile (64-byte swizzled K-major) and 64 x NT
+// byte B tiles, so the ring holds more stages.
+template <int NT, bool F8> struct TcCfg {
+    static constexpr int kElem = F8 ? 1 : 2;
+    static constexpr int kATileBytes = kWindowRows * kChunkCols * kElem;
+    static constexpr int kBoxCols = 128 / kElem; // N columns per 128-byte swizzle atom / TMA box
+    static constexpr int kStages = F8 ? (NT == 256 ? 6 : 8) : (NT == 256 ? 4 : NT == 128 ? 5 : 6);
+    static constexpr int kBTileBytes = kChunkCols * NT * kElem;
     static constexpr int kStage = kATileBytes + kBTileBytes;
     static constexpr int kStagingOff = kStages * kStage;
     static constexpr int kPendOff = kStagingOff + kStages * kStagingBytes; // int4 [kStages]: img, e0, e0a, e1
@@ -186,13 +200,14 @@ __device__ __forceinline__ int4 decode_item(const TcBatch &batch, int item)
 //   warps 6-9 (epilogue): per item wait "accum_full", tcgen05.ld the rows
 //     (warp w reads TMEM lanes 32 (w % 4) ..), alpha/beta, store to C[perm],
 //     arrive "accum_empty" -- overlapping the next item's main loop.
-template <int NT, typename OutT>
+template <int NT, typename OutT, bool F8>
 __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_constant__ TcBatch batch)
 {
-    using Cfg = TcCfg<NT>;
+    using Cfg = TcCfg<NT, F8>;
     constexpr int S = Cfg::kStages;
-    constexpr int kBoxes = NT / 64;       // 64-column boxes per B row slice
-    constexpr int kGathers = 16 * kBoxes; // gather4 instructions per condensed chunk
+    constexpr int kATileBytes = Cfg::kATileBytes;
+    constexpr int kBoxes = NT / Cfg::kBoxCols; // 128-byte-wide boxes per B row slice
+    constexpr int kGathers = 16 * kBoxes;      // gather4 instructions per condensed chunk
     extern __shared__ __align__(1024) uint8_t smem[];
     int4 *pend = reinterpret_cast<int4 *>(smem + Cfg::kPendOff);
     int4 *pend2 = reinterpret_cast<int4 *>(smem + Cfg::kPend2Off);
@@ -292,7 +307,7 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                 pend2[s] = make_int4((i == 0 ? 1 : 0) | (i == it.z - 1 ? 2 : 0), k & 1, k, 0);
                 mbar_expect_tx(&full[s], Cfg::kBTileBytes + (img >= 0 ? kATileBytes : 0));
                 if (img >= 0) {
-                    bulk_copy_g2s(a_s, a.images + (size_t)img * (kATileBytes / 2), kATileBytes, &full[s]);
+                    bulk_copy_g2s(a_s, a.images + (size_t)img * kATileBytes, kATileBytes, &full[s]);
                     mbar_arrive(&staged[s]);
                 } else if (e1 > e0) {
                     const uint32_t bytes = (uint32_t)(((e1 - e0a) * 4 + 15) & ~15);
@@ -309,7 +324,8 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             if (col0 >= 0 && col63 == col0 + kChunkCols - 1) {
                 // 64 contiguous B rows (direct chunks): one 8 KB tiled box per 64 columns
                 if (lane < kBoxes)
-                    tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * 64, col0, &full[s]);
+                    tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * Cfg::kBoxCols, col0,
+                               &full[s]);
             } else {
                 // condensed columns: gather q = lane, lane + 32, .. reads the 4 columns of lane q % 16
                 const int src = lane & 15;
@@ -319,7 +335,8 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                 const int y3 = __shfl_sync(0xffffffffu, cur.cols.w, src);
                 for (int q = lane; q < kGathers; q += 32) {
                     const int box = q >> 4;
-                    tma_gather4(b_s + box * (kChunkCols * 128) + src * 512, &a.tmap_b, n0 + box * 64, y0, y1, y2, y3,
+                    tma_gather4(b_s + box * (kChunkCols * 128) + src * 512, &a.tmap_b, n0 + box * Cfg::kBoxCols, y0,
+                                y1, y2, y3,
                                 &full[s]);
                 }
             }
@@ -360,7 +377,10 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                 const uint32_t *st = reinterpret_cast<const uint32_t *>(smem + Cfg::kStagingOff + s * kStagingBytes);
                 for (int e = pd.y + sid; e < pd.w; e += kScatterThreads) {
                     const uint32_t v = st[e - pd.z];
-                    *reinterpret_cast<uint16_t *>(At + swz128_offset(v >> 22, (v >> 16) & 63u)) =
+                    if constexpr (F8)
+                        At[swz64_offset(v >> 22, (v >> 16) & 63u)] = (uint8_t)(v & 0xffu);
+                    else
+                        *reinterpret_cast<uint16_t *>(At + swz128_offset(v >> 22, (v >> 16) & 63u)) =
                         (uint16_t)(v & 0xffffu);
                 }
                 fence_proxy_async();
@@ -372,7 +392,7 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     } else if (warp == kMmaWarp) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            constexpr uint32_t idesc = idesc_f16(NT);
+            constexpr uint32_t idesc = idesc_f16(NT); // E4M3 has format code 0 in kind::f8f6f4 as FP16 in kind::f16
             for (int g = 0;; g++) {
                 const int s = g % S;
                 if (!mbar_wait(&full[s], (g / S) & 1)) { ok = false; break; }
@@ -385,11 +405,22 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                 tc_fence_after();
                 const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
                 const uint32_t d = tmem + (uint32_t)(b * NT);
+                if constexpr (F8) {
+                    // 2 x K = 32: A rows of 64 bytes (64-byte swizzle, 8-row groups 512 bytes apart),
+                    // B k-rows of 128 bytes (128-byte swizzle, atoms along N 8 KB apart)
 #pragma unroll
-                for (int kk = 0; kk < kChunkCols / 16; kk++) {
-                    const uint64_t ad = smem_desc(a_s + kk * 32, 16, 1024);
-                    const uint64_t bd = smem_desc(b_s + kk * 2048, kChunkCols * 128, 1024);
-                    umma_f16(d, ad, bd, idesc, ((f.x & 1) && kk == 0) ? 0u : 1u);
+                    for (int kk = 0; kk < kChunkCols / 32; kk++) {
+                        const uint64_t ad = smem_desc(a_s + kk * 32, 16, 512, 4);
+                        const uint64_t bd = smem_desc(b_s + kk * 4096, kChunkCols * 128, 1024);
+                        umma_f8(d, ad, bd, idesc, ((f.x & 1) && kk == 0) ? 0u : 1u);
+                    }
+                } else {
+#pragma unroll
+                    for (int kk = 0; kk < kChunkCols / 16; kk++) {
+                        const uint64_t ad = smem_desc(a_s + kk * 32, 16, 1024);
+                        const uint64_t bd = smem_desc(b_s + kk * 2048, kChunkCols * 128, 1024);
+                        umma_f16(d, ad, bd, idesc, ((f.x & 1) && kk == 0) ? 0u : 1u);
+                    }
                 }
                 umma_commit(&empty[s]);
                 if (f.x & 2)
@@ -416,12 +447,20 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             if (!got) { ok = false; break; }
             tc_fence_after();
             OutT *Crow = out_row >= 0 ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
+            float sa = 1.f;
+            if constexpr (F8)
+                sa = (i < a.M) ? a.row_scale[i] : 0.f;
             for (int cb = 0; cb < NT / 16; cb++) {
                 const int n = n0 + cb * 16;
                 if (n >= a.N)
                     break; // uniform across the warp
                 uint32_t r[16];
                 tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * NT + cb * 16), r);
+                if constexpr (F8) { // dequantise: row scale x column scale
+                    float *f = reinterpret_cast<float *>(r);
+#pragma unroll
+                    for (int q = 0; q < 16; q++) f[q] *= sa * __ldg(a.col_scale + min(n + q, a.N - 1));
+                }
                 if (Crow) {
                     store8_out(Crow + n, reinterpret_cast<const float *>(r), a.alpha, a.beta);
                     if (n + 8 < a.N)
@@ -493,16 +532,30 @@ int make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT,
 {
     const tca_plan *p = sj.p;
     TcJob &j = *out;
-    TCA_TRY(encode_b_map(sj, p->K, 1, &j.tmap_b));
-    TCA_TRY(encode_b_map(sj, p->K, kChunkCols, &j.tmap_tile));
+    if (sj.f8) {
+        // E4M3 B (K x N bytes, row stride ldq): boxes of 128 columns
+        TCA_TRY(encode_tensor_map_2d(&j.tmap_b, CU_TENSOR_MAP_DATA_TYPE_UINT8, sj.Bq, (uint64_t)sj.N, (uint64_t)p->K,
+                                     (uint64_t)sj.ldq, 128, 1, CU_TENSOR_MAP_SWIZZLE_128B));
+        TCA_TRY(encode_tensor_map_2d(&j.tmap_tile, CU_TENSOR_MAP_DATA_TYPE_UINT8, sj.Bq, (uint64_t)sj.N,
+                                     (uint64_t)p->K, (uint64_t)sj.ldq, 128, kChunkCols, CU_TENSOR_MAP_SWIZZLE_128B));
+        j.entries = p->tile_entries_f8;
+        j.images = p->images_f8;
+        j.row_scale = p->row_scale;
+        j.col_scale = sj.col_scale;
+    } else {
+        TCA_TRY(encode_b_map(sj, p->K, 1, &j.tmap_b));
+        TCA_TRY(encode_b_map(sj, p->K, kChunkCols, &j.tmap_tile));
+        j.entries = p->tile_entries;
+        j.images = reinterpret_cast<const uint8_t *>(p->images);
+        j.row_scale = nullptr;
+        j.col_scale = nullptr;
+    }
     j.win_info = p->tc_win_info;
     j.tile_ptr = p->tile_ptr;
     j.win_cols = p->win_cols;
     j.img_idx = p->img_idx;
     j.perm = p->perm;
     j.p_row_ptr = p->p_row_ptr;
-    j.entries = p->tile_entries;
-    j.images = p->images;
     j.B = sj.B;
     j.C = sj.C;
     j.status = p->d_status;
@@ -517,43 +570,46 @@ int make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT,
     return TCA_OK;
 }
 
-template <int NT, typename OutT>
+template <int NT, typename OutT, bool F8>
 int launch_group(const TcBatch &b, cudaStream_t s)
 {
-    const int smem = TcCfg<NT>::kSmem;
-    TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int smem = TcCfg<NT, F8>::kSmem;
+    TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int total = b.item_start[b.n_jobs];
     const int grid = std::min(total, std::max(kSMs, (total + kMaxCtaItems - 1) / kMaxCtaItems));
-    spmm_tc_kernel<NT, OutT><<<grid, kThreads, smem, s>>>(b);
+    spmm_tc_kernel<NT, OutT, F8><<<grid, kThreads, smem, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
 }
 
-int launch_group_typed(const TcBatch &b, int NT, int c_dtype, cudaStream_t s)
+template <typename OutT>
+int launch_group_out(const TcBatch &b, int NT, bool f8, cudaStream_t s)
+{
+    if (f8)
+        return NT == 128 ? launch_group<128, OutT, true>(b, s) : launch_group<256, OutT, true>(b, s);
+    switch (NT) {
+    case 64: return launch_group<64, OutT, false>(b, s);
+    case 128: return launch_group<128, OutT, false>(b, s);
+    default: return launch_group<256, OutT, false>(b, s);
+    }
+}
+
+int launch_group_typed(const TcBatch &b, int NT, bool f8, int c_dtype, cudaStream_t s)
 {
     if (b.n_jobs == 0 || b.item_start[b.n_jobs] == 0)
         return TCA_OK;
-    if (c_dtype == TCA_DTYPE_F16) {
-        switch (NT) {
-        case 64: return launch_group<64, __half>(b, s);
-        case 128: return launch_group<128, __half>(b, s);
-        default: return launch_group<256, __half>(b, s);
-        }
-    }
-    switch (NT) {
-    case 64: return launch_group<64, float>(b, s);
-    case 128: return launch_group<128, float>(b, s);
-    default: return launch_group<256, float>(b, s);
-    }
+    return c_dtype == TCA_DTYPE_F16 ? launch_group_out<__half>(b, NT, f8, s) : launch_group_out<float>(b, NT, f8, s);
 }
 
 } // namespace
 
-int pick_tc_tile(int n_tc, int N, bool batched)
+int pick_tc_tile(int n_tc, int N, bool batched, bool f8)
 {
+    const int lo = f8 ? 128 : 64; // E4M3 B tiles are whole 128-byte swizzle atoms
     int NT = N <= 64 ? 64 : N <= 128 ? 128 : 256;
+    NT = std::max(NT, lo);
     if (!batched)
-        while (NT > 64 && (long long)n_tc * ((N + NT - 1) / NT) < kSMs)
+        while (NT > lo && (long long)n_tc * ((N + NT - 1) / NT) < kSMs)
             NT /= 2;
     return NT;
 }
@@ -562,23 +618,25 @@ int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
                    cudaStream_t s)
 {
     const int widths[3] = {64, 128, 256};
-    for (int NT : widths) {
-        TcBatch b;
-        b.n_jobs = 0;
-        b.item_start[0] = 0;
-        for (int i = 0; i < n_jobs; i++) {
-            const SpmmJob &sj = jobs[i];
-            if (!sj.tc || sj.n_tile != NT || sj.p->n_tc == 0 || sj.N <= 0)
-                continue;
-            TCA_TRY(make_job(sj, alpha, beta, flags, NT, &b.job[b.n_jobs]));
-            b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + sj.p->n_tc * b.job[b.n_jobs].ntiles;
-            b.n_jobs++;
-            if (b.n_jobs == kMaxJobs) {
-                TCA_TRY(launch_group_typed(b, NT, c_dtype, s));
-                b.n_jobs = 0;
+    for (bool f8 : {false, true}) {
+        for (int NT : widths) {
+            TcBatch b;
+            b.n_jobs = 0;
+            b.item_start[0] = 0;
+            for (int i = 0; i < n_jobs; i++) {
+                const SpmmJob &sj = jobs[i];
+                if (!sj.tc || sj.f8 != f8 || sj.n_tile != NT || sj.p->n_tc == 0 || sj.N <= 0)
+                    continue;
+                TCA_TRY(make_job(sj, alpha, beta, flags, NT, &b.job[b.n_jobs]));
+                b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + sj.p->n_tc * b.job[b.n_jobs].ntiles;
+                b.n_jobs++;
+                if (b.n_jobs == kMaxJobs) {
+                    TCA_TRY(launch_group_typed(b, NT, f8, c_dtype, s));
+                    b.n_jobs = 0;
+                }
             }
+            TCA_TRY(launch_group_typed(b, NT, f8, c_dtype, s));
         }
-        TCA_TRY(launch_group_typed(b, NT, c_dtype, s));
     }
     return TCA_OK;
 }

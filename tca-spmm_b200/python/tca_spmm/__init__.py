@@ -30,7 +30,10 @@ ARR_TC_WINDOWS, ARR_CC_WINDOWS, ARR_TILE_FIRST, ARR_WIN_COLS = 5, 6, 7, 8
 ARR_TILE_PTR, ARR_TILE_ENTRIES, ARR_TILE_SRC = 9, 10, 11
 ARR_TILE_IMAGE_IDX, ARR_TILE_IMAGES = 12, 13
 ARR_CC_ITEMS, ARR_ALL_ITEMS = 14, 15
-_ARR_DTYPE = {ARR_P_VAL: np.uint16, ARR_TILE_ENTRIES: np.uint32, ARR_TILE_IMAGES: np.uint16}
+ARR_ROW_SCALE, ARR_P_VAL_F8, ARR_TILE_ENTRIES_F8, ARR_TILE_IMAGES_F8 = 16, 17, 18, 19
+_ARR_DTYPE = {ARR_P_VAL: np.uint16, ARR_TILE_ENTRIES: np.uint32, ARR_TILE_IMAGES: np.uint16,
+              ARR_ROW_SCALE: np.float32, ARR_P_VAL_F8: np.uint8, ARR_TILE_ENTRIES_F8: np.uint32,
+              ARR_TILE_IMAGES_F8: np.uint8}
 
 STATUS = {
     0: "TCA_OK", 1: "TCA_ERR_INVALID_ARG", 2: "TCA_ERR_CUDA", 3: "TCA_ERR_ALLOC",
@@ -89,6 +92,10 @@ _SIGS = {
     "tca_sddmm": ([_VP, _P, _I, _P, _I, _I, _P, _I, _F, _VP], _I),
     "tca_spmm_t": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _VP], _I),
     "tca_plan_build_transpose": ([_VP, _VP], _I),
+    "tca_plan_quantize_fp8": ([_VP, _VP], _I),
+    "tca_quantize_b_fp8": ([_P, _I, _I, _I, _P, _I, _P, _VP], _I),
+    "tca_spmm_fp8": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP], _I),
+    "tca_spmm_fp8_batched": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _VP, ctypes.POINTER(_VP)], _I),
     "tca_spmm_host": ([_P, _P, _P, _I, _I, _I, _P, _I, _P, _I, _U, _I, ctypes.POINTER(ctypes.c_double)], _I),
 }
 
@@ -290,6 +297,21 @@ class Plan:
                                     _out_code(out.dtype), alpha, beta, _stream_handle(stream)))
         return out
 
+    def quantize_fp8(self, stream=None):
+        """Builds / refreshes the plan's E4M3 form of A (tca_plan_quantize_fp8)."""
+        _check(self._lib.tca_plan_quantize_fp8(self._h, _stream_handle(stream)))
+
+    def spmm_fp8(self, B, out=None, out_dtype=None, alpha=1.0, beta=0.0, keep_empty_rows=False, stream=None):
+        """E4M3 forward: A per-row and B per-column quantized, FP32 accumulation
+        (tca_spmm_fp8). B is float16; it is quantized per call."""
+        torch = _torch()
+        out_dtype = out_dtype or (out.dtype if out is not None else torch.float16)
+        N, out = _prepare_dense(B, out, self.M, out_dtype)
+        flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+        _check(self._lib.tca_spmm_fp8(self._h, _ptr(B), B.stride(0), N, _ptr(out), out.stride(0),
+                                      _out_code(out.dtype), alpha, beta, flags, _stream_handle(stream)))
+        return out
+
     def build_transpose(self, stream=None):
         _check(self._lib.tca_plan_build_transpose(self._h, _stream_handle(stream)))
 
@@ -326,6 +348,38 @@ def spmm_batched(plans, Bs, outs, alpha=1.0, beta=0.0, keep_empty_rows=False, n_
     flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
     _check(lib().tca_spmm_batched(arr, n, code, alpha, beta, flags, _stream_handle(stream), ev))
     return outs
+
+
+def spmm_fp8_batched(plans, Bs, outs, alpha=1.0, beta=0.0, keep_empty_rows=False, n_tile=0, events=None,
+                     stream=None):
+    """E4M3 forwards of many plans in a few launches (tca_spmm_fp8_batched);
+    every plan at most once."""
+    n = len(plans)
+    arr = (BatchItem * max(n, 1))()
+    for i, (p, B, C) in enumerate(zip(plans, Bs, outs)):
+        N, _ = _prepare_dense(B, C, p.M, C.dtype)
+        arr[i] = BatchItem(p.handle, _ptr(B), B.stride(0), N, _ptr(C), C.stride(0), n_tile)
+    code = _out_code(outs[0].dtype) if n else DTYPE_F16
+    ev = None
+    if events is not None:
+        ev = (_VP * 4)(*[(e.cuda_event if e is not None else None) for e in events])
+    flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+    _check(lib().tca_spmm_fp8_batched(arr, n, code, alpha, beta, flags, _stream_handle(stream), ev))
+    return outs
+
+
+def quantize_b_fp8(B, stream=None):
+    """B (K x N float16, CUDA) -> (Bq uint8 K x ldq, scale float32 N) with
+    ldq = N rounded up to 16 (tca_quantize_b_fp8)."""
+    torch = _torch()
+    if B.dim() != 2 or B.dtype != torch.float16 or B.stride(1) != 1:
+        raise ValueError("B must be a K x N float16 tensor with unit column stride")
+    K, N = B.shape
+    ldq = (N + 15) // 16 * 16
+    Bq = torch.zeros((K, ldq), dtype=torch.uint8, device=B.device)
+    scale = torch.empty(N, dtype=torch.float32, device=B.device)
+    _check(lib().tca_quantize_b_fp8(_ptr(B), B.stride(0), K, N, _ptr(Bq), ldq, _ptr(scale), _stream_handle(stream)))
+    return Bq, scale
 
 
 def spmm_host(row_ptr: np.ndarray, col_idx: np.ndarray, vals: np.ndarray, K: int, B: np.ndarray,
