@@ -268,6 +268,45 @@ def run_ours(args, world, rank):
     if tfile.exists():
         traffic = json.loads(tfile.read_text()).get(dominant)
 
+    # FP8-E4M3 forward of the same step (per-row A / per-column B scales; B is
+    # quantized inside every step), and the error of both precisions vs FP64
+    def step8():
+        tca_spmm.spmm_fp8_batched(plans, Bs, Cs)
+
+    for _ in range(args.warmup):
+        step8()
+    barrier(world)
+    e0.record()
+    for _ in range(args.steps):
+        step8()
+    e1.record()
+    barrier(world)
+    ms8 = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+    evs8 = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(n_prof)]
+    for e4 in evs8:  # torch only reads events it has recorded itself once
+        for e in e4:
+            e.record()
+    torch.cuda.synchronize()
+    for k in range(n_prof):
+        tca_spmm.spmm_fp8_batched(plans, Bs, Cs, events=evs8[k])
+    torch.cuda.synchronize()
+    fp8 = {"value": round(world * flops_step / (ms8 * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+           "ms_per_step": round(ms8, 5), "speedup_vs_fp16": round(ms_step / ms8, 3),
+           "kernels_us": {"spmm_tc_kernel_e4m3": round(float(np.mean([e[0].elapsed_time(e[1]) for e in evs8])) * 1e3, 3),
+                          "spmm_cc_stream_kernel_e4m3":
+                              round(float(np.mean([e[2].elapsed_time(e[3]) for e in evs8])) * 1e3, 3)},
+           "quantization": "E4M3, per-row A and per-column B FP32 scales, FP32 accumulation, FP16 out; "
+                           "B is quantized inside every step"}
+    if rank == 0 and not args.no_cpu:
+        from oracle import oracle
+        c0 = probs[0][0]
+        ref = oracle.spmm_f64(c0["row_ptr"], c0["col"], c0["vals"], c0["B"])
+        y16 = plans[0].spmm(Bs[0]).float().cpu().numpy()
+        y8 = plans[0].spmm_fp8(Bs[0]).float().cpu().numpy()
+        nrm = np.linalg.norm(ref)
+        fp8["rel_err_vs_f64"] = float(f"{np.linalg.norm(y8 - ref) / nrm:.4e}")
+        fp8["fp16_rel_err_vs_f64"] = float(f"{np.linalg.norm(y16 - ref) / nrm:.4e}")
+
     # e2e through the host-buffer entry point
     e2e_steps = max(1, min(args.steps, 8))
     pinned = []
@@ -313,6 +352,7 @@ def run_ours(args, world, rank):
                      "kernels_us": {"spmm_tc_kernel": round(tc_mean * 1e3, 3),
                                     "spmm_cc_stream_kernel": round(cc_mean * 1e3, 3)}},
         "e2e": e2e,
+        "fp8": fp8,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
     }

@@ -166,7 +166,8 @@ typedef struct tca_batch_item {
     int ldb, N;
     void *d_C;
     int ldc;
-    int n_tile;
+    int n_tile;   /* tensor-core N-slice width: 64, 128, 256 (E4M3: 128, 256); 0 = by N */
+    int cc_cols;  /* CUDA-core output columns per lane: 2, 4, 8; 0 = by N */
 } tca_batch_item_t;
 
 /* Forwards of many plans (layers of different shapes and sparsity) in a
@@ -224,6 +225,28 @@ TCA_API int tca_spmm_fp8(tca_plan_t plan, const void *d_B_f16, int ldb, int N, v
  * plan may appear once per batch. n_tile: 128 or 256 (0 = by N). */
 TCA_API int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
                                  unsigned flags, tca_stream_t stream, void *const *events);
+
+/* ---- Batched forward as a CUDA graph, and its autotuner (no counterpart in
+ * the reference: its launch geometry is fixed per call by workload_manager,
+ * src/our_spmm.cu:347-471) ---- */
+typedef enum { TCA_PRECISION_F16 = 0, TCA_PRECISION_E4M3 = 1 } tca_precision_t;
+typedef struct tca_graph *tca_graph_t;
+
+/* Captures tca_spmm_batched (precision F16) or tca_spmm_fp8_batched (E4M3)
+ * over `items` into a CUDA graph. Runs the batch once eagerly first (one-time
+ * set-up and validation; it writes the items' C), then captures a second run
+ * on a private stream. The graph keeps the items' pointers: replaying it after
+ * freeing any of them is undefined. */
+TCA_API int tca_batch_graph_create(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
+                                   unsigned flags, int precision, tca_graph_t *graph);
+/* One replay of the captured batch on `stream`. */
+TCA_API int tca_batch_graph_launch(tca_graph_t graph, tca_stream_t stream);
+TCA_API int tca_batch_graph_destroy(tca_graph_t graph);
+/* Per item, times every (n_tile, cc_cols) candidate on the item alone (median
+ * of `reps` runs, CUDA events on `stream`, synchronising) and stores the
+ * fastest into items[i].n_tile / items[i].cc_cols. Writes the items' C. */
+TCA_API int tca_batch_autotune(tca_batch_item_t *items, int n_items, int c_dtype, int precision, int reps,
+                               tca_stream_t stream);
 
 /* ------------------------------------------------------------------ */
 /* Host-side matrix I/O and format conversion. Arrays returned through

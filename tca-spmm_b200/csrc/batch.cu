@@ -1,0 +1,171 @@
+// batch.cu -- the batched forward as a CUDA graph, and its autotuner.
+//
+// A batch (many layers of different shapes, sparsity and N) runs as a few
+// persistent launches (tca_spmm_batched / tca_spmm_fp8_batched). The host
+// side of such a call -- argument checks, one TMA descriptor pair per item,
+// kernel-parameter blocks of up to 32 items -- costs more than the launches'
+// device time for small layers, so the batch is captured once into a CUDA
+// graph and replayed: a replay is one cudaGraphLaunch.
+//
+// The autotuner picks, per item, the tensor-core N-slice width (n_tile) and
+// the CUDA-core columns per lane (cc_cols) by timing each candidate on the
+// item alone with CUDA events (median of a few runs), and writes the winners
+// back into the items. The reference has neither (its launch geometry is fixed
+// by workload_manager, src/our_spmm.cu:347-471).
+#include <algorithm>
+#include <vector>
+#include "tca_internal.cuh"
+#include "plan.cuh"
+
+struct tca_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace tca {
+namespace {
+
+int run_batch(const tca_batch_item_t *items, int n, int c_dtype, float alpha, float beta, unsigned flags, int precision,
+              cudaStream_t s)
+{
+    return precision == TCA_PRECISION_E4M3
+               ? tca_spmm_fp8_batched(items, n, c_dtype, alpha, beta, flags, s, nullptr)
+               : tca_spmm_batched(items, n, c_dtype, alpha, beta, flags, s, nullptr);
+}
+
+struct StreamGuard {
+    cudaStream_t s = nullptr;
+    ~StreamGuard() { if (s) cudaStreamDestroy(s); }
+};
+
+} // namespace
+} // namespace tca
+
+using namespace tca;
+
+int tca_batch_graph_create(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
+                           unsigned flags, int precision, tca_graph_t *out)
+{
+    clear_error();
+    if (!out) return set_error(TCA_ERR_INVALID_ARG, "graph output pointer is NULL");
+    *out = nullptr;
+    if (precision != TCA_PRECISION_F16 && precision != TCA_PRECISION_E4M3)
+        return set_error(TCA_ERR_INVALID_ARG, "unknown precision %d", precision);
+    StreamGuard g;
+    TCA_CUDA_TRY(cudaStreamCreateWithFlags(&g.s, cudaStreamNonBlocking));
+    // One eager run first: it does the one-time work (kernel attributes, the
+    // E4M3 form of the plans, workspaces) that must not happen inside capture,
+    // and validates every item.
+    TCA_TRY(run_batch(items, n_items, c_dtype, alpha, beta, flags, precision, g.s));
+    TCA_CUDA_TRY(cudaStreamSynchronize(g.s));
+    cudaGraph_t graph = nullptr;
+    TCA_CUDA_TRY(cudaStreamBeginCapture(g.s, cudaStreamCaptureModeRelaxed));
+    const int st = run_batch(items, n_items, c_dtype, alpha, beta, flags, precision, g.s);
+    const cudaError_t ce = cudaStreamEndCapture(g.s, &graph);
+    if (st != TCA_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess)
+        return set_error(TCA_ERR_CUDA, "stream capture of the batch failed: %s", cudaGetErrorString(ce));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return set_error(TCA_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ie));
+    }
+    tca_graph *h = new tca_graph;
+    h->graph = graph;
+    h->exec = exec;
+    *out = h;
+    return TCA_OK;
+}
+
+int tca_batch_graph_launch(tca_graph_t g, tca_stream_t stream)
+{
+    clear_error();
+    if (!g) return set_error(TCA_ERR_INVALID_ARG, "graph is NULL");
+    TCA_CUDA_TRY(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return TCA_OK;
+}
+
+int tca_batch_graph_destroy(tca_graph_t g)
+{
+    clear_error();
+    if (!g) return TCA_OK;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return TCA_OK;
+}
+
+int tca_batch_autotune(tca_batch_item_t *items, int n_items, int c_dtype, int precision, int reps,
+                       tca_stream_t stream)
+{
+    clear_error();
+    if (n_items < 0 || (n_items > 0 && !items))
+        return set_error(TCA_ERR_INVALID_ARG, "invalid batch");
+    if (precision != TCA_PRECISION_F16 && precision != TCA_PRECISION_E4M3)
+        return set_error(TCA_ERR_INVALID_ARG, "unknown precision %d", precision);
+    reps = std::max(1, std::min(reps, 50));
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TCA_CUDA_TRY(cudaEventCreate(&e0));
+    const cudaError_t ee = cudaEventCreate(&e1);
+    if (ee != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return set_error(TCA_ERR_CUDA, "cudaEventCreate failed: %s", cudaGetErrorString(ee));
+    }
+    int status = TCA_OK;
+    // time one candidate: warm-up, then the median of `reps` runs of the item alone
+    auto time_item = [&](const tca_batch_item_t &it, float *us) -> int {
+        TCA_TRY(run_batch(&it, 1, c_dtype, 1.f, 0.f, 0, precision, s));
+        std::vector<float> t;
+        for (int r = 0; r < reps; r++) {
+            TCA_CUDA_TRY(cudaEventRecord(e0, s));
+            TCA_TRY(run_batch(&it, 1, c_dtype, 1.f, 0.f, 0, precision, s));
+            TCA_CUDA_TRY(cudaEventRecord(e1, s));
+            TCA_CUDA_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            TCA_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+            t.push_back(ms * 1000.f);
+        }
+        std::nth_element(t.begin(), t.begin() + t.size() / 2, t.end());
+        *us = t[t.size() / 2];
+        return TCA_OK;
+    };
+    for (int i = 0; i < n_items && status == TCA_OK; i++) {
+        tca_batch_item_t best = items[i];
+        float best_us = 3.4e38f;
+        const int N = items[i].N;
+        std::vector<int> tiles = precision == TCA_PRECISION_E4M3 ? std::vector<int>{128, 256}
+                                                                : std::vector<int>{64, 128, 256};
+        std::vector<int> cols = {2, 4, 8};
+        for (int nt : tiles) {
+            if (nt > 64 && nt / 2 >= N && !(precision == TCA_PRECISION_E4M3 && nt == 128))
+                continue; // a slice at least twice as wide as N only adds zero columns
+            for (int w : cols) {
+                if (w > 2 && w * 16 > N)
+                    continue; // fewer than half of the lanes would have columns
+                tca_batch_item_t cand = items[i];
+                cand.n_tile = nt;
+                cand.cc_cols = w;
+                float us = 0.f;
+                status = time_item(cand, &us);
+                if (status != TCA_OK)
+                    break;
+                if (us < best_us) {
+                    best_us = us;
+                    best = cand;
+                }
+            }
+            if (status != TCA_OK)
+                break;
+        }
+        if (status == TCA_OK)
+            items[i] = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return status;
+}

@@ -71,66 +71,99 @@ k_render_images_f8(const int *__restrict__ img_chunk, const int *__restrict__ ti
     }
 }
 
-// Column absolute maxima of B (as FP32 bit patterns, which order like the
-// non-negative values): thread = column, block row = 32 rows of B.
-__global__ void k_col_absmax(const __half *__restrict__ B, int ldb, int K, int N, unsigned *__restrict__ colmax)
+// B quantization of up to kMaxQJobs matrices per launch (blockIdx.z = matrix).
+constexpr int kMaxQJobs = 32;
+struct QJob {
+    const __half *B;
+    uint8_t *Bq;
+    unsigned *colmax; // column maxima as FP32 bit patterns, then the scales (in place)
+    int ldb, ldq, K, N;
+};
+struct QBatch {
+    int n;
+    QJob job[kMaxQJobs];
+};
+
+__global__ void k_col_zero(const __grid_constant__ QBatch b)
 {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= N)
-        return;
-    const int k0 = blockIdx.y * 32, k1 = min(K, k0 + 32);
-    float m = 0.f;
-    for (int k = k0; k < k1; k++) m = fmaxf(m, fabsf(__half2float(B[(size_t)k * ldb + n])));
-    atomicMax(colmax + n, __float_as_uint(m));
+    const QJob &q = b.job[blockIdx.z];
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < q.N; n += gridDim.x * blockDim.x) q.colmax[n] = 0u;
 }
 
-// Bq[k, n] = E4M3(B[k, n] / s[n]); thread = 4 consecutive columns of one row.
-__global__ void k_quant_cols(const __half *__restrict__ B, int ldb, int K, int N, const unsigned *__restrict__ colmax,
-                             uint8_t *__restrict__ Bq, int ldq)
+// Column absolute maxima (FP32 bit patterns order like the non-negative
+// values): thread = column, blockIdx.y = 32 rows of B.
+__global__ void k_col_absmax(const __grid_constant__ QBatch b)
 {
+    const QJob &q = b.job[blockIdx.z];
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k0 = blockIdx.y * 32;
+    if (n >= q.N || k0 >= q.K)
+        return;
+    const int k1 = min(q.K, k0 + 32);
+    float m = 0.f;
+    for (int k = k0; k < k1; k++) m = fmaxf(m, fabsf(__half2float(q.B[(size_t)k * q.ldb + n])));
+    atomicMax(q.colmax + n, __float_as_uint(m));
+}
+
+// Bq[k, n] = E4M3(B[k, n] / s[n]); thread = 4 consecutive columns, rows blockIdx.y, + gridDim.y, ...
+__global__ void k_quant_cols(const __grid_constant__ QBatch b)
+{
+    const QJob &q = b.job[blockIdx.z];
     const int n = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
-    if (n >= N)
+    if (n >= q.N)
         return;
     float s[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++) s[i] = n + i < N ? scale_of(__uint_as_float(colmax[n + i])) : 1.f;
-    for (int k = blockIdx.y; k < K; k += gridDim.y) {
+    for (int i = 0; i < 4; i++) s[i] = n + i < q.N ? scale_of(__uint_as_float(q.colmax[n + i])) : 1.f;
+    for (int k = blockIdx.y; k < q.K; k += gridDim.y) {
         uint32_t packed = 0;
 #pragma unroll
         for (int i = 0; i < 4; i++)
-            if (n + i < N)
-                packed |= (uint32_t)to_e4m3(__half2float(B[(size_t)k * ldb + n + i]) / s[i]) << (8 * i);
-        if (n + 4 <= N) {
-            *reinterpret_cast<uint32_t *>(Bq + (size_t)k * ldq + n) = packed;
+            if (n + i < q.N)
+                packed |= (uint32_t)to_e4m3(__half2float(q.B[(size_t)k * q.ldb + n + i]) / s[i]) << (8 * i);
+        uint8_t *dst = q.Bq + (size_t)k * q.ldq + n;
+        if (n + 4 <= q.N) {
+            *reinterpret_cast<uint32_t *>(dst) = packed;
         } else {
-            for (int i = 0; n + i < N; i++) Bq[(size_t)k * ldq + n + i] = (uint8_t)(packed >> (8 * i));
+            for (int i = 0; n + i < q.N; i++) dst[i] = (uint8_t)(packed >> (8 * i));
         }
     }
 }
 
-// colmax (bit patterns) -> scales, in place.
-__global__ void k_col_scale(unsigned *__restrict__ colmax, int N)
+// column maxima -> scales, in place
+__global__ void k_col_scale(const __grid_constant__ QBatch b)
 {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n < N) {
-        const float s = scale_of(__uint_as_float(colmax[n]));
-        colmax[n] = __float_as_uint(s);
-    }
+    const QJob &q = b.job[blockIdx.z];
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < q.N; n += gridDim.x * blockDim.x)
+        q.colmax[n] = __float_as_uint(scale_of(__uint_as_float(q.colmax[n])));
 }
 
 unsigned blocks(long long n, int per) { return (unsigned)((n + per - 1) / per); }
 
-int quantize_b(const __half *B, int ldb, int K, int N, uint8_t *Bq, int ldq, float *scale, cudaStream_t s)
+int quantize_b_batch(const QBatch &b, cudaStream_t s)
 {
-    if (K <= 0 || N <= 0)
+    int maxK = 0, maxN = 0;
+    for (int i = 0; i < b.n; i++) {
+        maxK = std::max(maxK, b.job[i].K);
+        maxN = std::max(maxN, b.job[i].N);
+    }
+    if (b.n == 0 || maxK == 0 || maxN == 0)
         return TCA_OK;
-    unsigned *colmax = reinterpret_cast<unsigned *>(scale);
-    TCA_CUDA_TRY(cudaMemsetAsync(colmax, 0, sizeof(unsigned) * (size_t)N, s));
-    k_col_absmax<<<dim3(blocks(N, 256), blocks(K, 32)), 256, 0, s>>>(B, ldb, K, N, colmax);
-    k_quant_cols<<<dim3(blocks(blocks(N, 4), 128), (unsigned)std::min(K, 65535)), 128, 0, s>>>(B, ldb, K, N, colmax, Bq, ldq);
-    k_col_scale<<<blocks(N, 256), 256, 0, s>>>(colmax, N);
+    const unsigned z = (unsigned)b.n;
+    k_col_zero<<<dim3(blocks(maxN, 256), 1, z), 256, 0, s>>>(b);
+    k_col_absmax<<<dim3(blocks(maxN, 256), blocks(maxK, 32), z), 256, 0, s>>>(b);
+    k_quant_cols<<<dim3(blocks(blocks(maxN, 4), 128), (unsigned)std::min(maxK, 65535), z), 128, 0, s>>>(b);
+    k_col_scale<<<dim3(blocks(maxN, 256), 1, z), 256, 0, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
+}
+
+int quantize_b(const __half *B, int ldb, int K, int N, uint8_t *Bq, int ldq, float *scale, cudaStream_t s)
+{
+    QBatch b;
+    b.n = 1;
+    b.job[0] = QJob{B, Bq, reinterpret_cast<unsigned *>(scale), ldb, ldq, K, N};
+    return quantize_b_batch(b, s);
 }
 
 int quantize_plan(tca_plan *p, cudaStream_t s)
@@ -187,8 +220,10 @@ int plan_workspace(tca_plan *p, int N, uint8_t **Bq, int *ldq, float **scale)
     return TCA_OK;
 }
 
+// The E4M3 job of one forward; B's quantization is appended to `qb` (flushed
+// by the caller) when given, else run here.
 int make_fp8_job(tca_plan_t p, const void *B, int ldb, int N, void *C, int ldc, int c_dtype, bool batched,
-                 cudaStream_t s, SpmmJob *job)
+                 cudaStream_t s, SpmmJob *job, QBatch *qb)
 {
     if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
     TCA_TRY(check_dense_args(B, ldb, N, C, ldc, c_dtype, p->M, p->K));
@@ -213,7 +248,16 @@ int make_fp8_job(tca_plan_t p, const void *B, int ldb, int N, void *C, int ldc, 
     float *scale;
     int ldq;
     TCA_TRY(plan_workspace(p, N, &Bq, &ldq, &scale));
-    TCA_TRY(quantize_b((const __half *)B, ldb, p->K, N, Bq, ldq, scale, s));
+    const QJob q{(const __half *)B, Bq, reinterpret_cast<unsigned *>(scale), ldb, ldq, p->K, N};
+    if (qb) {
+        if (qb->n == kMaxQJobs) {
+            TCA_TRY(quantize_b_batch(*qb, s));
+            qb->n = 0;
+        }
+        qb->job[qb->n++] = q;
+    } else {
+        TCA_TRY(quantize_b(q.B, ldb, p->K, N, Bq, ldq, scale, s));
+    }
     job->Bq = Bq;
     job->ldq = ldq;
     job->col_scale = scale;
@@ -271,7 +315,7 @@ int tca_spmm_fp8(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, i
     clear_error();
     cudaStream_t s = (cudaStream_t)stream;
     SpmmJob job;
-    TCA_TRY(make_fp8_job(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, false, s, &job));
+    TCA_TRY(make_fp8_job(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, false, s, &job, nullptr));
     if (p->M == 0 || N == 0) return TCA_OK;
     if (p->K == 0) // no nonzeros can exist: A B = 0
         return tca_spmm(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, alpha, beta, flags, stream);
@@ -289,6 +333,8 @@ int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype
     cudaStream_t s = (cudaStream_t)stream;
     std::vector<SpmmJob> jobs;
     jobs.reserve((size_t)n_items);
+    QBatch qb;
+    qb.n = 0;
     for (int i = 0; i < n_items; i++) {
         const tca_batch_item_t &it = items[i];
         for (int k = 0; k < i; k++)
@@ -296,14 +342,16 @@ int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype
                 return set_error(TCA_ERR_INVALID_ARG,
                                  "batch items %d and %d share a plan: an E4M3 batch quantizes B into the plan", k, i);
         SpmmJob j;
-        TCA_TRY(make_fp8_job(it.plan, it.d_B_f16, it.ldb, it.N, it.d_C, it.ldc, c_dtype, true, s, &j));
+        TCA_TRY(make_fp8_job(it.plan, it.d_B_f16, it.ldb, it.N, it.d_C, it.ldc, c_dtype, true, s, &j, &qb));
         if (it.n_tile == 128 || it.n_tile == 256)
             j.n_tile = it.n_tile;
+        j.cc_w = it.cc_cols;
         if (it.plan->M > 0 && it.N > 0 && it.plan->K == 0) // no nonzeros can exist: A B = 0
             TCA_TRY(tca_spmm(it.plan, it.d_B_f16, it.ldb, it.N, it.d_C, it.ldc, c_dtype, alpha, beta, flags, stream));
         else if (it.plan->M > 0 && it.N > 0)
             jobs.push_back(j);
     }
+    TCA_TRY(quantize_b_batch(qb, s));
     auto rec = [&](int i) -> int {
         if (events && events[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[i], s));
         return TCA_OK;

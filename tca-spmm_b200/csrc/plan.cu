@@ -742,6 +742,7 @@ int tca_spmm_batched(const tca_batch_item_t *items, int n_items, int c_dtype, fl
         TCA_TRY(make_job(it.plan, it.d_B_f16, it.ldb, it.N, it.d_C, it.ldc, c_dtype, true, &j));
         if (it.n_tile == 64 || it.n_tile == 128 || it.n_tile == 256)
             j.n_tile = it.n_tile;
+        j.cc_w = it.cc_cols;
         if (it.plan->M > 0 && it.N > 0)
             jobs.push_back(j);
     }

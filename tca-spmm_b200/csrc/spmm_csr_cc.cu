@@ -750,7 +750,7 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
                 continue;
             // E4M3 jobs always qualify (B is the library's own aligned copy; C was checked)
             const bool vec = sj.f8 || vec_ok(sj.B, sj.ldb, sj.N, sj.C, sj.ldc, c_dtype);
-            const int lpr = vec ? pick_w(sj.N) : 32;
+            const int lpr = vec ? (sj.cc_w == 2 || sj.cc_w == 4 || sj.cc_w == 8 ? sj.cc_w : pick_w(sj.N)) : 32;
             if (lpr != kd[0] || (vec ? 1 : 0) != kd[1] || (sj.f8 ? 1 : 0) != kd[2])
                 continue;
             CcJob &a = b.job[b.n_jobs];

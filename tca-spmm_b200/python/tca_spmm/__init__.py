@@ -67,7 +67,8 @@ class PlanInfo(ctypes.Structure):
 
 class BatchItem(ctypes.Structure):
     _fields_ = [("plan", ctypes.c_void_p), ("d_B_f16", ctypes.c_void_p), ("ldb", ctypes.c_int),
-                ("N", ctypes.c_int), ("d_C", ctypes.c_void_p), ("ldc", ctypes.c_int), ("n_tile", ctypes.c_int)]
+                ("N", ctypes.c_int), ("d_C", ctypes.c_void_p), ("ldc", ctypes.c_int), ("n_tile", ctypes.c_int),
+                ("cc_cols", ctypes.c_int)]
 
 
 _lib = None
@@ -96,6 +97,10 @@ _SIGS = {
     "tca_quantize_b_fp8": ([_P, _I, _I, _I, _P, _I, _P, _VP], _I),
     "tca_spmm_fp8": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP], _I),
     "tca_spmm_fp8_batched": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _VP, ctypes.POINTER(_VP)], _I),
+    "tca_batch_graph_create": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _I, ctypes.POINTER(_VP)], _I),
+    "tca_batch_graph_launch": ([_VP, _VP], _I),
+    "tca_batch_graph_destroy": ([_VP], _I),
+    "tca_batch_autotune": ([ctypes.POINTER(BatchItem), _I, _I, _I, _I, _VP], _I),
     "tca_spmm_host": ([_P, _P, _P, _I, _I, _I, _P, _I, _P, _I, _U, _I, ctypes.POINTER(ctypes.c_double)], _I),
 }
 
@@ -366,6 +371,61 @@ def spmm_fp8_batched(plans, Bs, outs, alpha=1.0, beta=0.0, keep_empty_rows=False
     flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
     _check(lib().tca_spmm_fp8_batched(arr, n, code, alpha, beta, flags, _stream_handle(stream), ev))
     return outs
+
+
+PRECISION_F16, PRECISION_E4M3 = 0, 1
+_PRECISIONS = {"f16": PRECISION_F16, "fp16": PRECISION_F16, "e4m3": PRECISION_E4M3, "fp8": PRECISION_E4M3}
+
+
+def _batch_items(plans, Bs, outs, n_tiles=None, cc_cols=None):
+    n = len(plans)
+    arr = (BatchItem * max(n, 1))()
+    for i, (p, B, C) in enumerate(zip(plans, Bs, outs)):
+        N, _ = _prepare_dense(B, C, p.M, C.dtype)
+        arr[i] = BatchItem(p.handle, _ptr(B), B.stride(0), N, _ptr(C), C.stride(0),
+                           (n_tiles[i] if n_tiles else 0), (cc_cols[i] if cc_cols else 0))
+    return arr
+
+
+def autotune(plans, Bs, outs, precision="f16", reps=5, stream=None):
+    """Per item, the fastest (n_tile, cc_cols) by timing every candidate on the
+    item alone (tca_batch_autotune). Overwrites `outs`."""
+    arr = _batch_items(plans, Bs, outs)
+    code = _out_code(outs[0].dtype) if plans else DTYPE_F16
+    _check(lib().tca_batch_autotune(arr, len(plans), code, _PRECISIONS[precision], reps, _stream_handle(stream)))
+    return [(arr[i].n_tile, arr[i].cc_cols) for i in range(len(plans))]
+
+
+class BatchGraph:
+    """A batch of forwards (many layers) captured once as a CUDA graph
+    (tca_batch_graph_create) and replayed with launch(). Holds references to
+    the plans and tensors, whose addresses the graph keeps."""
+
+    def __init__(self, plans, Bs, outs, alpha=1.0, beta=0.0, keep_empty_rows=False, precision="f16",
+                 n_tiles=None, cc_cols=None):
+        self._keep = (list(plans), list(Bs), list(outs))
+        self._lib = lib()
+        arr = _batch_items(plans, Bs, outs, n_tiles, cc_cols)
+        code = _out_code(outs[0].dtype) if plans else DTYPE_F16
+        flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+        h = _VP()
+        _check(self._lib.tca_batch_graph_create(arr, len(plans), code, alpha, beta, flags, _PRECISIONS[precision],
+                                                ctypes.byref(h)))
+        self._h = h
+
+    def launch(self, stream=None):
+        _check(self._lib.tca_batch_graph_launch(self._h, _stream_handle(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.tca_batch_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def quantize_b_fp8(B, stream=None):
