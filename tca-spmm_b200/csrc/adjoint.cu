@@ -155,7 +155,8 @@ unsigned blocks_of(long long n, int per) { return (unsigned)((n + per - 1) / per
 
 struct Tmp {
     void *p = nullptr;
-    ~Tmp() { if (p) cudaFree(p); }
+    cudaStream_t s = nullptr;
+    ~Tmp() { if (p) dev_free(p, s); }
 };
 
 int build_transpose(tca_plan *p, cudaStream_t s)
@@ -164,18 +165,19 @@ int build_transpose(tca_plan *p, cudaStream_t s)
         return TCA_OK;
     const int M = p->M, K = p->K, nnz = p->nnz;
     Tmp tk, tk2, tv, tv2, tcount, trp, tcol, tcub;
+    for (Tmp *t : {&tk, &tk2, &tv, &tv2, &tcount, &trp, &tcol, &tcub}) t->s = s;
     unsigned long long *keys = nullptr, *keys2 = nullptr;
     int *order = nullptr, *order2 = nullptr, *count = nullptr, *t_rp = nullptr, *t_col = nullptr;
     const size_t n1 = nnz > 0 ? nnz : 1;
-    TCA_CUDA_TRY(cudaMalloc(&keys, sizeof(unsigned long long) * n1)); tk.p = keys;
-    TCA_CUDA_TRY(cudaMalloc(&keys2, sizeof(unsigned long long) * n1)); tk2.p = keys2;
-    TCA_CUDA_TRY(cudaMalloc(&order, sizeof(int) * n1)); tv.p = order;
-    TCA_CUDA_TRY(cudaMalloc(&order2, sizeof(int) * n1)); tv2.p = order2;
-    TCA_CUDA_TRY(cudaMalloc(&count, sizeof(int) * (size_t)(K + 1))); tcount.p = count;
-    TCA_CUDA_TRY(cudaMalloc(&t_rp, sizeof(int) * (size_t)(K + 1))); trp.p = t_rp;
-    TCA_CUDA_TRY(cudaMalloc(&t_col, sizeof(int) * n1)); tcol.p = t_col;
-    TCA_CUDA_TRY(cudaMalloc(&p->t_src, sizeof(int) * n1));
-    TCA_CUDA_TRY(cudaMalloc(&p->t_vals, sizeof(__half) * n1));
+    TCA_TRY(dev_malloc((void **)&keys, sizeof(unsigned long long) * n1, s)); tk.p = keys;
+    TCA_TRY(dev_malloc((void **)&keys2, sizeof(unsigned long long) * n1, s)); tk2.p = keys2;
+    TCA_TRY(dev_malloc((void **)&order, sizeof(int) * n1, s)); tv.p = order;
+    TCA_TRY(dev_malloc((void **)&order2, sizeof(int) * n1, s)); tv2.p = order2;
+    TCA_TRY(dev_malloc((void **)&count, sizeof(int) * (size_t)(K + 1), s)); tcount.p = count;
+    TCA_TRY(dev_malloc((void **)&t_rp, sizeof(int) * (size_t)(K + 1), s)); trp.p = t_rp;
+    TCA_TRY(dev_malloc((void **)&t_col, sizeof(int) * n1, s)); tcol.p = t_col;
+    TCA_TRY(dev_malloc((void **)&p->t_src, sizeof(int) * n1, s));
+    TCA_TRY(dev_malloc((void **)&p->t_vals, sizeof(__half) * n1, s));
     TCA_CUDA_TRY(cudaMemsetAsync(count, 0, sizeof(int) * (size_t)(K + 1), s));
     if (M > 0)
         k_transpose_keys<<<blocks_of((long long)M * 32, 256), 256, 0, s>>>(p->perm, p->p_row_ptr, p->p_col, p->src,
@@ -184,12 +186,13 @@ int build_transpose(tca_plan *p, cudaStream_t s)
         size_t tmp = 0;
         TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys, keys2, order, order2, nnz, 0, 64, s));
         void *tb;
-        TCA_CUDA_TRY(cudaMalloc(&tb, tmp > 0 ? tmp : 1)); tcub.p = tb;
+        TCA_TRY(dev_malloc((void **)&tb, tmp > 0 ? tmp : 1, s)); tcub.p = tb;
         TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tb, tmp, keys, keys2, order, order2, nnz, 0, 64, s));
         // values in A^T order come from the plan's values mapped back to the caller's order
         __half *vals_caller;
         Tmp tvc;
-        TCA_CUDA_TRY(cudaMalloc(&vals_caller, sizeof(__half) * n1)); tvc.p = vals_caller;
+        tvc.s = s;
+        TCA_TRY(dev_malloc((void **)&vals_caller, sizeof(__half) * n1, s)); tvc.p = vals_caller;
         // p_val[k] is the value of caller index src[k]: scatter it back
         // (src is a permutation, so the scatter has no conflicts)
         k_scatter_half<<<blocks_of(nnz, 256), 256, 0, s>>>(p->src, p->p_val, vals_caller, nnz);
@@ -202,8 +205,9 @@ int build_transpose(tca_plan *p, cudaStream_t s)
         size_t tmp = 0;
         TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, count, t_rp, K + 1, s));
         Tmp tb;
+        tb.s = s;
         void *b;
-        TCA_CUDA_TRY(cudaMalloc(&b, tmp > 0 ? tmp : 1)); tb.p = b;
+        TCA_TRY(dev_malloc((void **)&b, tmp > 0 ? tmp : 1, s)); tb.p = b;
         TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(b, tmp, count, t_rp, K + 1, s));
         TCA_CUDA_TRY(cudaStreamSynchronize(s));
     }
@@ -288,8 +292,8 @@ int transpose_update_values(tca_plan *p, const __half *vals, cudaStream_t s)
 void transpose_free(tca_plan *p)
 {
     if (p->tplan) tca_plan_destroy(p->tplan);
-    if (p->t_src) cudaFree(p->t_src);
-    if (p->t_vals) cudaFree(p->t_vals);
+    if (p->t_src) dev_free(p->t_src, nullptr);
+    if (p->t_vals) dev_free(p->t_vals, nullptr);
     p->tplan = nullptr;
     p->t_src = nullptr;
     p->t_vals = nullptr;

@@ -3,10 +3,58 @@
 // forward. The kernels live in spmm_*.cu and plan.cu.
 #include <cstring>
 #include <string>
+#include <map>
+#include <mutex>
 #include "tca_internal.cuh"
 #include "plan.cuh"
 
 namespace tca {
+
+namespace {
+std::mutex g_pool_mutex;
+std::map<int, cudaMemPool_t> g_pools;
+
+int pool_of_current_device(cudaMemPool_t *out)
+{
+    int dev = 0;
+    TCA_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) {
+        *out = it->second;
+        return TCA_OK;
+    }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    TCA_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = UINT64_MAX; // freed blocks stay in the pool for the next plan
+    TCA_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[dev] = pool;
+    *out = pool;
+    return TCA_OK;
+}
+} // namespace
+
+int dev_malloc(void **ptr, size_t bytes, cudaStream_t s)
+{
+    cudaMemPool_t pool;
+    TCA_TRY(pool_of_current_device(&pool));
+    const cudaError_t e = cudaMallocFromPoolAsync(ptr, bytes > 0 ? bytes : 16, pool, s);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return set_error(TCA_ERR_ALLOC, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return TCA_OK;
+}
+
+void dev_free(void *ptr, cudaStream_t s)
+{
+    if (ptr)
+        cudaFreeAsync(ptr, s);
+}
 
 static thread_local char g_err[1024] = "";
 
@@ -111,11 +159,11 @@ int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals
     };
     do {
         cudaError_t e;
-        if ((e = cudaMalloc(&d_rp, sizeof(int) * (size_t)(M + 1))) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
-        if ((e = cudaMalloc(&d_ci, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1))) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
-        if ((e = cudaMalloc(&d_v, 2 * (size_t)(nnz > 0 ? nnz : 1))) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
-        if ((e = cudaMalloc(&d_B, 2 * (size_t)(K > 0 ? K : 1) * N)) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
-        if ((e = cudaMalloc(&d_C, c_elem * (size_t)M * N)) != cudaSuccess) { fail_cuda(e, "cudaMalloc"); break; }
+        if ((st = dev_malloc((void **)&d_rp, sizeof(int) * (size_t)(M + 1), nullptr)) != TCA_OK) break;
+        if ((st = dev_malloc((void **)&d_ci, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1), nullptr)) != TCA_OK) break;
+        if ((st = dev_malloc((void **)&d_v, 2 * (size_t)(nnz > 0 ? nnz : 1), nullptr)) != TCA_OK) break;
+        if ((st = dev_malloc((void **)&d_B, 2 * (size_t)(K > 0 ? K : 1) * N, nullptr)) != TCA_OK) break;
+        if ((st = dev_malloc(&d_C, c_elem * (size_t)M * N, nullptr)) != TCA_OK) break;
         if ((e = cudaMemcpy(d_rp, h_row_ptr, sizeof(int) * (size_t)(M + 1), cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
         if (nnz > 0) {
             if ((e = cudaMemcpy(d_ci, h_col_idx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
@@ -144,11 +192,8 @@ int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals
     if (plan) tca_plan_destroy(plan);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    cudaFree(d_rp);
-    cudaFree(d_ci);
-    cudaFree(d_v);
-    cudaFree(d_B);
-    cudaFree(d_C);
+    for (void *ptr : {(void *)d_rp, (void *)d_ci, (void *)d_v, (void *)d_B, d_C})
+        if (ptr) dev_free(ptr, nullptr);
     return st;
 }
 

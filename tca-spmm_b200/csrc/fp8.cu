@@ -170,9 +170,7 @@ int quantize_plan(tca_plan *p, cudaStream_t s)
 {
     if (!p->row_scale) {
         auto alloc = [&](void **ptr, size_t b) -> int {
-            const cudaError_t e = cudaMalloc(ptr, b > 0 ? b : 16);
-            if (e != cudaSuccess)
-                return set_error(TCA_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+            TCA_TRY(dev_malloc(ptr, b, s));
             p->bytes += b;
             return TCA_OK;
         };
@@ -203,14 +201,14 @@ int plan_workspace(tca_plan *p, int N, uint8_t **Bq, int *ldq, float **scale)
     const size_t need = bq + sizeof(float) * (size_t)q;
     if (need > p->fp8_ws_bytes) {
         if (p->fp8_ws) {
-            cudaFree(p->fp8_ws); // synchronises with work that still reads it
+            TCA_CUDA_TRY(cudaDeviceSynchronize()); // queued work on any stream may still read it
+            dev_free(p->fp8_ws, nullptr);
             p->bytes -= p->fp8_ws_bytes;
             p->fp8_ws = nullptr;
             p->fp8_ws_bytes = 0;
         }
-        const cudaError_t e = cudaMalloc(&p->fp8_ws, need);
-        if (e != cudaSuccess)
-            return set_error(TCA_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", need, cudaGetErrorString(e));
+        TCA_TRY(dev_malloc(&p->fp8_ws, need, nullptr));
+        TCA_CUDA_TRY(cudaStreamSynchronize(nullptr)); // usable from every stream
         p->fp8_ws_bytes = need;
         p->bytes += need;
     }
@@ -275,7 +273,7 @@ void plan_free_fp8(tca_plan *p)
 {
     void *arrs[] = {p->row_scale, p->p_val_f8, p->tile_entries_f8, p->images_f8, p->fp8_ws};
     for (void *a : arrs)
-        if (a) cudaFree(a);
+        if (a) dev_free(a, nullptr);
     p->row_scale = nullptr;
     p->p_val_f8 = nullptr;
     p->tile_entries_f8 = nullptr;
@@ -319,9 +317,7 @@ int tca_spmm_fp8(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, i
     if (p->M == 0 || N == 0) return TCA_OK;
     if (p->K == 0) // no nonzeros can exist: A B = 0
         return tca_spmm(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, alpha, beta, flags, stream);
-    TCA_TRY(launch_tc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
-    TCA_TRY(launch_cc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
-    return TCA_OK;
+    return run_jobs_with_events(&job, 1, c_dtype, alpha, beta, flags, s, nullptr);
 }
 
 int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
@@ -352,15 +348,5 @@ int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype
             jobs.push_back(j);
     }
     TCA_TRY(quantize_b_batch(qb, s));
-    auto rec = [&](int i) -> int {
-        if (events && events[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[i], s));
-        return TCA_OK;
-    };
-    TCA_TRY(rec(0));
-    TCA_TRY(launch_tc_jobs(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s));
-    TCA_TRY(rec(1));
-    TCA_TRY(rec(2));
-    TCA_TRY(launch_cc_jobs(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s));
-    TCA_TRY(rec(3));
-    return TCA_OK;
+    return run_jobs_with_events(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s, events);
 }

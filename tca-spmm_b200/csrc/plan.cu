@@ -93,6 +93,26 @@ __global__ void k_permute(const int *__restrict__ perm, const int *__restrict__ 
     }
 }
 
+// Sets the bit of every column of p_col[lo, hi) in the shared bitmap. Eight
+// coalesced loads per thread are issued before their atomics, so that the
+// loop is not one memory latency per column.
+__device__ __forceinline__ void mark_columns(const int *__restrict__ p_col, int lo, int hi, uint32_t *bm)
+{
+    constexpr int U = 8;
+    for (int j0 = lo + threadIdx.x; j0 < hi; j0 += blockDim.x * U) {
+        int c[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int j = j0 + u * (int)blockDim.x;
+            c[u] = j < hi ? __ldg(p_col + j) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (c[u] >= 0)
+                atomicOr(&bm[c[u] >> 5], 1u << (c[u] & 31));
+    }
+}
+
 // 3. Window statistics: one block per window, K-bit bitmap in shared memory.
 __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
                                const int *__restrict__ p_sorted, int M, int K, int *__restrict__ win_nu,
@@ -107,10 +127,7 @@ __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__r
     __syncthreads();
     const int r0 = w * kWindowRows, r1 = min(M, r0 + kWindowRows);
     const int lo = p_row_ptr[r0], hi = p_row_ptr[r1];
-    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-        const int c = p_col[j];
-        atomicOr(&bm[c >> 5], 1u << (c & 31));
-    }
+    mark_columns(p_col, lo, hi, bm);
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
         if (!p_sorted[i]) atomicAnd(&s_elig, 0);
     __syncthreads();
@@ -175,10 +192,7 @@ k_tile_fill(const int4 *__restrict__ win_info, const long long *__restrict__ ent
 
     for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
     __syncthreads();
-    for (int j = lo + threadIdx.x; j < hi; j += blockDim.x) {
-        const int c = p_col[j];
-        atomicOr(&bm[c >> 5], 1u << (c & 31));
-    }
+    mark_columns(p_col, lo, hi, bm);
     __syncthreads();
     if (wi.w) { // direct window: every column < K of each touched 64-column block
         for (int b = threadIdx.x; 2 * b < nwords; b += blockDim.x) {
@@ -220,16 +234,20 @@ k_tile_fill(const int4 *__restrict__ win_info, const long long *__restrict__ ent
     if (i < r1) { cur = p_row_ptr[i]; end = p_row_ptr[i + 1]; }
     long long base = entry_base[t];
     for (int c = 0; c < nch; c++) {
+        // the row's columns in this chunk: ranks are increasing along the row and
+        // a chunk holds at most 64 of them -- binary search in [cur, cur + 64)
         const int lim = (c + 1) * kChunkCols;
-        int cnt = 0;
-        while (cur + cnt < end) {
-            const int col = p_col[cur + cnt];
+        int a = cur, b = min(end, cur + kChunkCols);
+        while (a < b) {
+            const int mid = (a + b) >> 1;
+            const int col = p_col[mid];
             const int rk = pre[col >> 5] + __popc(bm[col >> 5] & ((1u << (col & 31)) - 1u));
-            if (rk >= lim) break;
-            cnt++;
+            if (rk < lim) a = mid + 1; else b = mid;
         }
+        const int cnt = a - cur;
         int total;
         const int off = block_exclusive_scan128(cnt, &total, scratch);
+#pragma unroll 8
         for (int e = 0; e < cnt; e++) {
             const int j = cur + e;
             const int col = p_col[j];
@@ -281,18 +299,27 @@ k_render_images(const int *__restrict__ img_chunk, const int *__restrict__ tile_
 
 unsigned blocks_for(long long n, int per) { return (unsigned)((n + per - 1) / per); }
 
+// The stream a plan is being built on: temporaries and plan arrays are
+// stream-ordered allocations on it.
+thread_local cudaStream_t tl_build_stream = nullptr;
+
+struct BuildStream {
+    cudaStream_t prev;
+    explicit BuildStream(cudaStream_t s) : prev(tl_build_stream) { tl_build_stream = s; }
+    ~BuildStream() { tl_build_stream = prev; }
+};
+
 struct DevBuf {
     void *p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
+    cudaStream_t s = tl_build_stream;
+    ~DevBuf() { if (p) dev_free(p, s); }
 };
 
 template <typename T>
 int dev_alloc(T **ptr, size_t count, size_t *bytes)
 {
     const size_t b = sizeof(T) * (count > 0 ? count : 1);
-    cudaError_t e = cudaMalloc((void **)ptr, b);
-    if (e != cudaSuccess)
-        return set_error(TCA_ERR_ALLOC, "cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+    TCA_TRY(dev_malloc((void **)ptr, b, tl_build_stream));
     if (bytes) *bytes += b;
     return TCA_OK;
 }
@@ -300,6 +327,7 @@ int dev_alloc(T **ptr, size_t count, size_t *bytes)
 void free_plan(tca_plan *p)
 {
     if (!p) return;
+    cudaDeviceSynchronize(); // the plan's arrays may still be read by queued work on any stream
     transpose_free(p);
     plan_free_fp8(p);
     void *arrs[] = {p->perm, p->p_row_ptr, p->p_col, p->p_val, p->src, p->tc_windows, p->cc_windows,
@@ -307,7 +335,7 @@ void free_plan(tca_plan *p)
                     p->img_idx, p->images, p->img_chunk, p->cc_items, p->all_items, p->tc_win_info,
                     p->d_status};
     for (void *a : arrs)
-        if (a) cudaFree(a);
+        if (a) dev_free(a, nullptr);
     delete p;
 }
 
@@ -341,6 +369,7 @@ void build_items(const std::vector<int> &windows, const std::vector<int> &row_pt
 
 int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *val, cudaStream_t s)
 {
+    BuildStream build_stream(s);
     const int M = p->M, K = p->K, nnz = p->nnz;
     size_t *bytes = &p->bytes;
     DevBuf t_row_nnz, t_row_sorted, t_err, t_iota, t_keys_out, t_p_sorted, t_scan_in, t_cub;
@@ -543,6 +572,27 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
 } // namespace
 } // namespace tca
 
+namespace tca {
+int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
+                         cudaStream_t s, void *const *events)
+{
+    LaunchList tc, cc;
+    TCA_TRY(launch_tc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &tc));
+    TCA_TRY(launch_cc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &cc));
+    auto rec = [&](int i) -> int {
+        if (events && events[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[i], s));
+        return TCA_OK;
+    };
+    TCA_TRY(rec(0));
+    for (auto &f : tc) TCA_TRY(f(s));
+    TCA_TRY(rec(1));
+    TCA_TRY(rec(2));
+    for (auto &f : cc) TCA_TRY(f(s));
+    TCA_TRY(rec(3));
+    return TCA_OK;
+}
+} // namespace tca
+
 using namespace tca;
 
 extern "C" {
@@ -703,17 +753,7 @@ static int spmm_impl(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_
     SpmmJob job;
     TCA_TRY(make_job(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, false, &job));
     if (p->M == 0 || N == 0) return TCA_OK;
-    auto rec = [&](int i) -> int {
-        if (ev && ev[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)ev[i], s));
-        return TCA_OK;
-    };
-    TCA_TRY(rec(0));
-    TCA_TRY(launch_tc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
-    TCA_TRY(rec(1));
-    TCA_TRY(rec(2));
-    TCA_TRY(launch_cc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
-    TCA_TRY(rec(3));
-    return TCA_OK;
+    return run_jobs_with_events(&job, 1, c_dtype, alpha, beta, flags, s, ev);
 }
 
 int tca_spmm(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype, float alpha,
@@ -746,19 +786,11 @@ int tca_spmm_batched(const tca_batch_item_t *items, int n_items, int c_dtype, fl
         if (it.plan->M > 0 && it.N > 0)
             jobs.push_back(j);
     }
-    cudaStream_t s = (cudaStream_t)stream;
-    auto rec = [&](int i) -> int {
-        if (events && events[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[i], s));
-        return TCA_OK;
-    };
-    TCA_TRY(rec(0));
-    TCA_TRY(launch_tc_jobs(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s));
-    TCA_TRY(rec(1));
-    TCA_TRY(rec(2));
-    TCA_TRY(launch_cc_jobs(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s));
-    TCA_TRY(rec(3));
-    return TCA_OK;
+    return run_jobs_with_events(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, (cudaStream_t)stream,
+                                events);
 }
+
+
 
 int tca_plan_launch_counts(tca_plan_t p, int N, int *n_tc_launches, int *n_cc_launches)
 {

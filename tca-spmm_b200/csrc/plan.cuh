@@ -25,6 +25,8 @@
 //                      swizzled K-major layout the tensor cores read from
 //                      shared memory; img_idx is -1 for the other chunks
 #pragma once
+#include <functional>
+#include <vector>
 #include "tca_internal.cuh"
 
 struct tca_plan {
@@ -128,15 +130,26 @@ struct SpmmJob {
     const float *col_scale = nullptr;
 };
 
+// Kernel launches whose host-side preparation (argument blocks, TMA
+// descriptors) is already done: running one only launches.
+using LaunchList = std::vector<std::function<int(cudaStream_t)>>;
+
 // Tensor-core (tcgen05) forward over the tensor-core windows of every job
-// (jobs with tc set), in as few launches as the N-slice widths allow.
+// (jobs with tc set), in as few launches as the N-slice widths allow. With
+// `defer` the prepared launches are appended to it instead of issued.
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s);
+                   cudaStream_t s, LaunchList *defer = nullptr);
 
 // CUDA-core forward over the remaining windows of every job (all windows of
 // jobs without tc), in as few launches as the row widths allow.
 int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s);
+                   cudaStream_t s, LaunchList *defer = nullptr);
+
+// Prepares both launch lists, then issues them with optional events (4
+// caller-created cudaEvent_t or NULL) around the tensor-core and the
+// CUDA-core launches, so that the events bracket device work only.
+int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
+                         cudaStream_t s, void *const *events);
 
 // The N-slice width a single forward of this plan uses.
 int pick_tc_tile(int n_tc, int N, bool batched, bool f8 = false);

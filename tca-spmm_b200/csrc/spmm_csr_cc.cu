@@ -18,6 +18,7 @@
 // Malformed CSR never faults: row ranges are clamped to [0, nnz] and
 // nonzeros whose column is outside [0, K) contribute nothing.
 #include <algorithm>
+#include <memory>
 #include <vector>
 #include <cuda_fp8.h>
 #include "tca_internal.cuh"
@@ -727,7 +728,7 @@ int launch_cc_typed(const CcBatch &b, int w, bool vec, bool f8, cudaStream_t s)
 } // namespace
 
 int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s)
+                   cudaStream_t s, LaunchList *defer)
 {
     // groups: (columns per lane, vectorised, E4M3) -- stream kernel with 2/4/8 columns, scalar items
     const int kinds[7][3] = {{2, 1, 0}, {4, 1, 0}, {8, 1, 0}, {32, 0, 0}, {2, 1, 1}, {4, 1, 1}, {8, 1, 1}};
@@ -737,10 +738,23 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
         b.block_start[0] = 0;
         b.item_start[0] = 0;
         auto flush = [&]() -> int {
-            const int st = (c_dtype == TCA_DTYPE_F16) ? launch_cc_typed<__half>(b, kd[0], kd[1] != 0, kd[2] != 0, s)
-                                                      : launch_cc_typed<float>(b, kd[0], kd[1] != 0, kd[2] != 0, s);
+            if (b.n_jobs == 0)
+                return TCA_OK;
+            const int w = kd[0];
+            const bool vec = kd[1] != 0, f8 = kd[2] != 0;
+            auto run = [c_dtype, w, vec, f8](const CcBatch &bb, cudaStream_t st) {
+                return (c_dtype == TCA_DTYPE_F16) ? launch_cc_typed<__half>(bb, w, vec, f8, st)
+                                                  : launch_cc_typed<float>(bb, w, vec, f8, st);
+            };
+            int status = TCA_OK;
+            if (defer) {
+                auto held = std::make_shared<CcBatch>(b);
+                defer->push_back([held, run](cudaStream_t st) { return run(*held, st); });
+            } else {
+                status = run(b, s);
+            }
             b.n_jobs = 0;
-            return st;
+            return status;
         };
         for (int i = 0; i < n_jobs; i++) {
             const SpmmJob &sj = jobs[i];

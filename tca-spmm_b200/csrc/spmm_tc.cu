@@ -36,6 +36,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <algorithm>
+#include <memory>
 #include <mutex>
 #include "tca_internal.cuh"
 #include "plan.cuh"
@@ -615,9 +616,18 @@ int pick_tc_tile(int n_tc, int N, bool batched, bool f8)
 }
 
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s)
+                   cudaStream_t s, LaunchList *defer)
 {
     const int widths[3] = {64, 128, 256};
+    auto emit = [&](const TcBatch &b, int NT, bool f8) -> int {
+        if (b.n_jobs == 0 || b.item_start[b.n_jobs] == 0)
+            return TCA_OK;
+        if (!defer)
+            return launch_group_typed(b, NT, f8, c_dtype, s);
+        auto held = std::make_shared<TcBatch>(b);
+        defer->push_back([held, NT, f8, c_dtype](cudaStream_t st) { return launch_group_typed(*held, NT, f8, c_dtype, st); });
+        return TCA_OK;
+    };
     for (bool f8 : {false, true}) {
         for (int NT : widths) {
             TcBatch b;
@@ -631,11 +641,11 @@ int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
                 b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + sj.p->n_tc * b.job[b.n_jobs].ntiles;
                 b.n_jobs++;
                 if (b.n_jobs == kMaxJobs) {
-                    TCA_TRY(launch_group_typed(b, NT, f8, c_dtype, s));
+                    TCA_TRY(emit(b, NT, f8));
                     b.n_jobs = 0;
                 }
             }
-            TCA_TRY(launch_group_typed(b, NT, f8, c_dtype, s));
+            TCA_TRY(emit(b, NT, f8));
         }
     }
     return TCA_OK;

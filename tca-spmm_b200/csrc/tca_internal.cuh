@@ -35,6 +35,13 @@ void clear_error();
 
 inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+// Device memory of the library (api.cu): stream-ordered allocations from a
+// per-device memory pool that keeps freed memory for reuse (plan builds and
+// host-buffer calls allocate and free dozens of arrays per call; plain
+// cudaMalloc / cudaFree cost ~60 us each and cudaFree synchronises the device).
+int dev_malloc(void **ptr, size_t bytes, cudaStream_t s);
+void dev_free(void *ptr, cudaStream_t s);
+
 // Checks the dense operands of a forward (api.cu).
 int check_dense_args(const void *B, int ldb, int N, const void *C, int ldc, int c_dtype, int M, int K);
 
