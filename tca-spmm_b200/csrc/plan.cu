@@ -9,12 +9,20 @@
 // atomics), so a host restatement reproduces it bit for bit:
 //   1. check the CSR, count each row, flag rows with strictly increasing columns;
 //   2. order rows by nnz (descending, ties by row index) and re-order the CSR;
-//   3. per 128-row window: distinct columns (a shared-memory bitmap), nnz,
-//      eligibility (all rows strictly increasing);
-//   4. on the host: a window goes to tensor cores when it is eligible and
-//      nnz_w >= tc_min_density * 128 * 64 * ceil(distinct_w / 64);
-//   5. per tensor-core window: condensed column list and per-chunk nonzero
-//      entries packed as (local_row << 22 | local_col << 16 | fp16 bits).
+//   3. per 128-row window: distinct columns and touched 64-column blocks of K
+//      (a shared-memory bitmap), nnz, eligibility (all rows strictly
+//      increasing);
+//   4. on the host: a window's chunks are its touched 64-column blocks
+//      ("direct": B rows contiguous) when there are at most twice as many of
+//      them as chunks of its distinct columns, else its distinct columns 64
+//      at a time ("condensed"); it goes to tensor cores when it is eligible
+//      and nnz_w >= tc_min_density * 128 * 64 * chunks_w;
+//   5. per tensor-core window: its chunk columns (one block per window), then
+//      per chunk (one block each) the nonzeros of every row inside the chunk
+//      -- counted, prefix-summed into tile_ptr, written as entries packed
+//      (local_row << 22 | local_col << 16 | fp16 bits) ordered by (row, col);
+//   6. dense 16 KB images of the chunks with >= 2048 entries; CUDA-core
+//      work items (host).
 #include <cub/cub.cuh>
 #include <vector>
 #include <algorithm>
@@ -95,7 +103,8 @@ __global__ void k_permute(const int *__restrict__ perm, const int *__restrict__ 
 
 // Sets the bit of every column of p_col[lo, hi) in the shared bitmap. Eight
 // coalesced loads per thread are issued before their atomics, so that the
-// loop is not one memory latency per column.
+// loop is not one memory latency per column. A bit is only ever set, so a
+// stale read costs at most one redundant atomic.
 __device__ __forceinline__ void mark_columns(const int *__restrict__ p_col, int lo, int hi, uint32_t *bm)
 {
     constexpr int U = 8;
@@ -107,9 +116,15 @@ __device__ __forceinline__ void mark_columns(const int *__restrict__ p_col, int 
             c[u] = j < hi ? __ldg(p_col + j) : -1;
         }
 #pragma unroll
-        for (int u = 0; u < U; u++)
-            if (c[u] >= 0)
-                atomicOr(&bm[c[u] >> 5], 1u << (c[u] & 31));
+        for (int u = 0; u < U; u++) {
+            // dense windows set the same few words over and over: skip the
+            // (serialising) shared atomic when the bit is already there
+            if (c[u] >= 0) {
+                const uint32_t bit = 1u << (c[u] & 31);
+                if (!(*(volatile uint32_t *)&bm[c[u] >> 5] & bit))
+                    atomicOr(&bm[c[u] >> 5], bit);
+            }
+        }
     }
 }
 
@@ -147,10 +162,11 @@ __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__r
     }
 }
 
-// Block-wide exclusive scan of one int per thread (blockDim.x == 128).
-__device__ int block_exclusive_scan128(int v, int *total, int *scratch /* >= 5 ints */)
+// Block-wide exclusive scan of one int per thread (blockDim.x a multiple of
+// 32, at most 1024); *total gets the sum. scratch holds >= 33 ints.
+__device__ int block_exclusive_scan(int v, int *total, int *scratch)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     int x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -161,31 +177,29 @@ __device__ int block_exclusive_scan128(int v, int *total, int *scratch /* >= 5 i
     __syncthreads();
     if (threadIdx.x == 0) {
         int run = 0;
-        for (int k = 0; k < 4; k++) { const int t = scratch[k]; scratch[k] = run; run += t; }
-        scratch[4] = run;
+        for (int k = 0; k < nw; k++) { const int t = scratch[k]; scratch[k] = run; run += t; }
+        scratch[32] = run;
     }
     __syncthreads();
     const int res = x - v + scratch[warp];
-    *total = scratch[4];
+    *total = scratch[32];
     __syncthreads();
     return res;
 }
 
-// 5. Tile fill: one block of 128 threads per tensor-core window.
-__global__ void __launch_bounds__(128)
-k_tile_fill(const int4 *__restrict__ win_info, const long long *__restrict__ entry_base,
-            const int *__restrict__ p_row_ptr,
-            const int *__restrict__ p_col, const __half *__restrict__ p_val, int M, int K,
-            int *__restrict__ win_cols, int *__restrict__ tile_ptr, uint32_t *__restrict__ entries,
-            int *__restrict__ tile_src)
+// 5a. Window columns: one block of 1024 threads per tensor-core window builds
+// the window's column bitmap (expanded to whole 64-column blocks for a direct
+// window) and writes its columns, ascending, 64 per chunk, -1 padding.
+__global__ void __launch_bounds__(1024)
+k_tile_cols(const int4 *__restrict__ win_info, const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
+            int M, int K, int *__restrict__ win_cols)
 {
     extern __shared__ uint32_t sm[];
-    __shared__ int scratch[8];
+    __shared__ int scratch[33];
     const int nwords = (K + 31) >> 5;
     uint32_t *bm = sm;
     int *pre = reinterpret_cast<int *>(sm + nwords);
-    const int t = blockIdx.x;
-    const int4 wi = win_info[t];
+    const int4 wi = win_info[blockIdx.x];
     const int w = wi.x, c0 = wi.y, nch = wi.z;
     const int r0 = w * kWindowRows, r1 = min(M, r0 + kWindowRows);
     const int lo = p_row_ptr[r0], hi = p_row_ptr[r1];
@@ -206,15 +220,14 @@ k_tile_fill(const int4 *__restrict__ win_info, const long long *__restrict__ ent
         __syncthreads();
     }
     // exclusive prefix of popcounts over words: each thread owns a contiguous segment
-    const int seg = (nwords + 127) / 128;
+    const int seg = (nwords + blockDim.x - 1) / blockDim.x;
     const int wb = min(nwords, (int)threadIdx.x * seg), we = min(nwords, wb + seg);
     int local = 0;
     for (int i = wb; i < we; i++) local += __popc(bm[i]);
     int nu;
-    int run = block_exclusive_scan128(local, &nu, scratch);
+    int run = block_exclusive_scan(local, &nu, scratch);
     for (int i = wb; i < we; i++) { pre[i] = run; run += __popc(bm[i]); }
     __syncthreads();
-    // condensed column list (ascending), padded with -1 to a multiple of 64
     int *wc = win_cols + (size_t)c0 * kChunkCols;
     for (int i = threadIdx.x; i < nwords; i += blockDim.x) {
         uint32_t b = bm[i];
@@ -226,41 +239,94 @@ k_tile_fill(const int4 *__restrict__ win_info, const long long *__restrict__ ent
         }
     }
     for (int k = nu + threadIdx.x; k < nch * kChunkCols; k += blockDim.x) wc[k] = -1;
+}
 
-    // per chunk: each thread owns one local row and walks its sorted columns
-    const int lr = threadIdx.x;
-    const int i = r0 + lr;
-    int cur = 0, end = 0;
-    if (i < r1) { cur = p_row_ptr[i]; end = p_row_ptr[i + 1]; }
-    long long base = entry_base[t];
-    for (int c = 0; c < nch; c++) {
-        // the row's columns in this chunk: ranks are increasing along the row and
-        // a chunk holds at most 64 of them -- binary search in [cur, cur + 64)
-        const int lim = (c + 1) * kChunkCols;
-        int a = cur, b = min(end, cur + kChunkCols);
-        while (a < b) {
-            const int mid = (a + b) >> 1;
-            const int col = p_col[mid];
-            const int rk = pre[col >> 5] + __popc(bm[col >> 5] & ((1u << (col & 31)) - 1u));
-            if (rk < lim) a = mid + 1; else b = mid;
-        }
-        const int cnt = a - cur;
-        int total;
-        const int off = block_exclusive_scan128(cnt, &total, scratch);
-#pragma unroll 8
-        for (int e = 0; e < cnt; e++) {
-            const int j = cur + e;
-            const int col = p_col[j];
-            const int rk = pre[col >> 5] + __popc(bm[col >> 5] & ((1u << (col & 31)) - 1u)) - c * kChunkCols;
-            const uint32_t bits = __half_as_ushort(p_val[j]);
-            entries[base + off + e] = ((uint32_t)lr << 22) | ((uint32_t)rk << 16) | bits;
-            tile_src[base + off + e] = j;
-        }
-        if (threadIdx.x == 0) tile_ptr[c0 + c] = (int)base;
-        base += total;
-        cur += cnt;
+// First position in the sorted columns p_col[a, b) whose column is >= v.
+__device__ __forceinline__ int lower_bound_col(const int *__restrict__ p_col, int a, int b, int v)
+{
+    while (a < b) {
+        const int mid = (a + b) >> 1;
+        if (p_col[mid] < v) a = mid + 1; else b = mid;
     }
-    if (threadIdx.x == 0) tile_ptr[c0 + nch] = (int)base;
+    return a;
+}
+
+// The nonzeros of local row lr of chunk c of window wi are p_col[*lo, *hi):
+// the row's columns from the chunk's first column up to the next chunk's
+// first column (a chunk holds at most 64 columns of a row).
+__device__ __forceinline__ void chunk_row_range(const int4 &wi, int c, int lr, const int *__restrict__ p_row_ptr,
+                                                const int *__restrict__ p_col, const int *__restrict__ wc, int M,
+                                                int *lo, int *hi)
+{
+    const int i = wi.x * kWindowRows + lr;
+    *lo = *hi = 0;
+    if (i >= M)
+        return;
+    const int rs = p_row_ptr[i], re = p_row_ptr[i + 1];
+    const int first = wc[c * kChunkCols];
+    const int next = c + 1 < wi.z ? wc[(c + 1) * kChunkCols] : 0x7fffffff;
+    *lo = lower_bound_col(p_col, rs, re, first);
+    *hi = lower_bound_col(p_col, *lo, min(re, *lo + kChunkCols), next);
+}
+
+// 5b. Nonzeros per chunk: one block of 128 threads (= rows) per chunk.
+__global__ void __launch_bounds__(128)
+k_tile_count(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_info,
+             const int *__restrict__ p_row_ptr, const int *__restrict__ p_col, const int *__restrict__ win_cols,
+             int M, int *__restrict__ chunk_nnz)
+{
+    __shared__ int scratch[33];
+    const int2 cw = chunk_win[blockIdx.x];
+    const int4 wi = win_info[cw.x];
+    const int *wc = win_cols + (size_t)wi.y * kChunkCols;
+    int lo, hi;
+    chunk_row_range(wi, cw.y, threadIdx.x, p_row_ptr, p_col, wc, M, &lo, &hi);
+    int total;
+    block_exclusive_scan(hi - lo, &total, scratch);
+    if (threadIdx.x == 0)
+        chunk_nnz[blockIdx.x] = total;
+}
+
+// 5c. Entries of each chunk, ordered by (row, column): one block per chunk;
+// tile_ptr (the exclusive sum of chunk_nnz) gives the chunk's first entry.
+__global__ void __launch_bounds__(128)
+k_tile_write(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_info,
+             const int *__restrict__ p_row_ptr, const int *__restrict__ p_col, const __half *__restrict__ p_val,
+             const int *__restrict__ win_cols, const int *__restrict__ tile_ptr, int M,
+             uint32_t *__restrict__ entries, int *__restrict__ tile_src)
+{
+    __shared__ int scratch[33];
+    __shared__ int s_cols[kChunkCols];
+    const int2 cw = chunk_win[blockIdx.x];
+    const int4 wi = win_info[cw.x];
+    const int *wc = win_cols + (size_t)wi.y * kChunkCols;
+    if (threadIdx.x < kChunkCols)
+        s_cols[threadIdx.x] = wc[cw.y * kChunkCols + threadIdx.x];
+    int lo, hi;
+    chunk_row_range(wi, cw.y, threadIdx.x, p_row_ptr, p_col, wc, M, &lo, &hi);
+    int total;
+    const int off = block_exclusive_scan(hi - lo, &total, scratch); // its barriers also publish s_cols
+    const long long base = (long long)tile_ptr[blockIdx.x] + off;
+    const int first = s_cols[0];
+    const uint32_t lr = threadIdx.x;
+#pragma unroll 4
+    for (int j = lo; j < hi; j++) {
+        const int col = p_col[j];
+        int rk;
+        if (wi.w) {
+            rk = col - first; // direct chunk: 64 consecutive columns
+        } else {             // condensed chunk: position among its ascending columns (-1 padding last)
+            int a = 0, b = kChunkCols;
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                const int v = s_cols[mid];
+                if (v >= 0 && v < col) a = mid + 1; else b = mid;
+            }
+            rk = a;
+        }
+        entries[base + (j - lo)] = (lr << 22) | ((uint32_t)rk << 16) | (uint32_t)__half_as_ushort(p_val[j]);
+        tile_src[base + (j - lo)] = j;
+    }
 }
 
 __global__ void k_update_p_val(const int *__restrict__ src, const __half *__restrict__ vals, __half *__restrict__ p_val, int n)
@@ -448,7 +514,7 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         TCA_TRY(dev_alloc(&d_el, W, nullptr)); t_el.p = d_el;
         const size_t smem = sizeof(uint32_t) * ((K + 31) / 32);
         TCA_CUDA_TRY(cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_window_stats<<<W, 256, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, d_nu, d_wn, d_el, d_nb);
+        k_window_stats<<<W, 1024, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, d_nu, d_wn, d_el, d_nb);
         TCA_CUDA_TRY(cudaGetLastError());
         TCA_CUDA_TRY(cudaMemcpyAsync(h_nu.data(), d_nu, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
         TCA_CUDA_TRY(cudaMemcpyAsync(h_nnz.data(), d_wn, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
@@ -463,8 +529,7 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     // at most twice the chunks of condensing its distinct columns (gathered
     // B rows); otherwise condensed.
     std::vector<int> tc_list, cc_list, h_first(1, 0), h_direct;
-    std::vector<long long> h_ebase;
-    long long ebase = 0;
+    long long ebase = 0; // nonzeros of the tensor-core windows so far
     for (int w = 0; w < W; w++) {
         const int nch_cond = (h_nu[w] + kChunkCols - 1) / kChunkCols;
         const bool direct = h_nblk[w] <= 2 * nch_cond;
@@ -480,7 +545,6 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
             tc_list.push_back(w);
             h_direct.push_back(direct ? 1 : 0);
             h_first.push_back(h_first.back() + nch);
-            h_ebase.push_back(ebase);
             ebase += h_nnz[w];
         } else {
             cc_list.push_back(w);
@@ -512,16 +576,31 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     TCA_CUDA_TRY(cudaMemsetAsync(p->tile_entries + p->tc_nnz, 0, sizeof(uint32_t) * kEntryPad, s));
     TCA_TRY(dev_alloc(&p->tile_src, (size_t)p->tc_nnz, bytes));
     if (p->n_tc > 0) {
-        DevBuf t_eb;
-        long long *d_eb;
-        TCA_TRY(dev_alloc(&d_eb, p->n_tc, nullptr)); t_eb.p = d_eb;
-        TCA_CUDA_TRY(cudaMemcpyAsync(d_eb, h_ebase.data(), sizeof(long long) * p->n_tc, cudaMemcpyHostToDevice, s));
+        // chunk -> (tensor-core window, chunk within the window)
+        std::vector<int2> h_cw;
+        h_cw.reserve((size_t)p->n_tc_chunks);
+        for (int t = 0; t < p->n_tc; t++)
+            for (int c = 0; c < h_wi[t].z; c++) h_cw.push_back(make_int2(t, c));
+        DevBuf t_cw, t_cn, t_scan;
+        int2 *d_cw;
+        int *d_cn;
+        TCA_TRY(dev_alloc(&d_cw, (size_t)p->n_tc_chunks, nullptr)); t_cw.p = d_cw;
+        TCA_TRY(dev_alloc(&d_cn, (size_t)p->n_tc_chunks + 1, nullptr)); t_cn.p = d_cn;
+        TCA_CUDA_TRY(cudaMemcpyAsync(d_cw, h_cw.data(), sizeof(int2) * h_cw.size(), cudaMemcpyHostToDevice, s));
+        TCA_CUDA_TRY(cudaMemsetAsync(d_cn + p->n_tc_chunks, 0, sizeof(int), s));
         const size_t smem = 2 * sizeof(uint32_t) * ((K + 31) / 32);
-        TCA_CUDA_TRY(cudaFuncSetAttribute(k_tile_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tile_fill<<<p->n_tc, 128, smem, s>>>(p->tc_win_info, d_eb, p->p_row_ptr, p->p_col, p->p_val,
-                                               M, K, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src);
+        TCA_CUDA_TRY(cudaFuncSetAttribute(k_tile_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_tile_cols<<<p->n_tc, 1024, smem, s>>>(p->tc_win_info, p->p_row_ptr, p->p_col, M, K, p->win_cols);
+        k_tile_count<<<p->n_tc_chunks, 128, 0, s>>>(d_cw, p->tc_win_info, p->p_row_ptr, p->p_col, p->win_cols, M,
+                                                    d_cn);
+        size_t tmp = 0;
+        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_cn, p->tile_ptr, p->n_tc_chunks + 1, s));
+        void *tb;
+        TCA_TRY(dev_alloc((char **)&tb, tmp, nullptr)); t_scan.p = tb;
+        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tb, tmp, d_cn, p->tile_ptr, p->n_tc_chunks + 1, s));
+        k_tile_write<<<p->n_tc_chunks, 128, 0, s>>>(d_cw, p->tc_win_info, p->p_row_ptr, p->p_col, p->p_val,
+                                                    p->win_cols, p->tile_ptr, M, p->tile_entries, p->tile_src);
         TCA_CUDA_TRY(cudaGetLastError());
-        TCA_CUDA_TRY(cudaStreamSynchronize(s)); // d_eb is freed at scope exit
     } else {
         TCA_CUDA_TRY(cudaMemsetAsync(p->tile_ptr, 0, sizeof(int), s));
     }
