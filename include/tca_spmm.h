@@ -226,6 +226,26 @@ TCA_API int tca_spmm_fp8(tca_plan_t plan, const void *d_B_f16, int ldb, int N, v
 TCA_API int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
                                  unsigned flags, tca_stream_t stream, void *const *events);
 
+/* tca_spmm_fp8 for callers that may not allocate device memory: those whose
+ * memory is handed out by someone else (a framework's own caching allocator,
+ * a fixed per-process budget) and those on a latency-critical path where a
+ * cudaMalloc / cudaFree, which may synchronise the device, is not allowed.
+ * This entry point has no counterpart in the reference.
+ * Instead of the plan's workspace it quantizes B into one fixed array of
+ * TCA_FP8_STATIC_SCRATCH_BYTES, part of the library on every GPU that loads
+ * it (held until the process exits). Limit: K * round_up(N, 16) bytes, rounded
+ * up to 256, plus 4 * round_up(N, 16) must fit; larger B is rejected with
+ * TCA_ERR_INVALID_ARG (use tca_spmm_fp8). The plan's E4M3 form must exist
+ * already (tca_plan_quantize_fp8, which allocates, called once at set-up).
+ * The first call on each device looks up the array's device address; make
+ * that first call before any stream capture. Every call on a device shares
+ * the one array (the call clears what it needs cleared): calls whose work
+ * overlaps on the GPU -- on different streams, or from different threads --
+ * race and give wrong results. Otherwise as tca_spmm_fp8. */
+#define TCA_FP8_STATIC_SCRATCH_BYTES (16u << 20)
+TCA_API int tca_spmm_fp8_static(tca_plan_t plan, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype,
+                                float alpha, float beta, unsigned flags, tca_stream_t stream);
+
 /* ---- Batched forward as a CUDA graph, and its autotuner (no counterpart in
  * the reference: its launch geometry is fixed per call by workload_manager,
  * src/our_spmm.cu:347-471) ---- */

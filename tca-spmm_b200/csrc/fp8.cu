@@ -12,6 +12,7 @@
 // rebuild, checked against a CPU restatement of the same quantization.
 #include <cuda_fp8.h>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 #include "tca_internal.cuh"
 #include "plan.cuh"
@@ -349,4 +350,103 @@ int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int c_dtype
     }
     TCA_TRY(quantize_b_batch(qb, s));
     return run_jobs_with_events(jobs.data(), (int)jobs.size(), c_dtype, alpha, beta, flags, s, events);
+}
+
+// ---------------------------------------------------------------------------
+// tca_spmm_fp8_static: the E4M3 forward with no allocation at all.
+//
+// tca_spmm_fp8 quantizes B into a workspace that it allocates on first use
+// and grows when N grows. Some callers cannot let it: their device memory is
+// handed out by someone else (a framework's own caching allocator, a fixed
+// per-process budget), or they sit on a latency-critical path where a
+// cudaMalloc / cudaFree -- which may synchronise the whole device -- is not
+// allowed. This entry point quantizes B into a fixed scratch array instead:
+// g_fp8_scratch, below, allocated with the library's module on every GPU that
+// loads it and held until the process exits.
+//
+// Layout of the scratch for one call: Bq (K rows of ldq = N rounded up to 16
+// bytes), rounded up to 256 bytes, then ldq FP32 words that first hold the
+// column maxima (cleared by the call itself) and then the column scales.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_fp8_scratch[TCA_FP8_STATIC_SCRATCH_BYTES];
+
+namespace tca {
+namespace {
+
+constexpr int kMaxDevices = 64;
+void *g_scratch_addr[kMaxDevices]; // device address of g_fp8_scratch, per device ordinal
+std::mutex g_scratch_mutex;
+
+// Device address of the scratch on the current device. The array's name in
+// host code is only a host-side handle of the symbol; the address a kernel
+// can use comes from cudaGetSymbolAddress, asked once per device with that
+// device current (the first call on each device).
+int static_scratch(void **out)
+{
+    int dev = 0;
+    TCA_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices)
+        return set_error(TCA_ERR_UNSUPPORTED, "device ordinal %d beyond the %d this entry point tracks", dev, kMaxDevices);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_fp8_scratch);
+        if (e != cudaSuccess || !p)
+            return set_error(TCA_ERR_CUDA, "cudaGetSymbolAddress of the static E4M3 scratch failed: %s",
+                             cudaGetErrorString(e));
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
+    return TCA_OK;
+}
+
+} // namespace
+} // namespace tca
+
+int tca_spmm_fp8_static(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype,
+                        float alpha, float beta, unsigned flags, tca_stream_t stream)
+{
+    clear_error();
+    if (!p) return set_error(TCA_ERR_INVALID_ARG, "plan is NULL");
+    TCA_TRY(check_dense_args(d_B_f16, ldb, N, d_C, ldc, c_dtype, p->M, p->K));
+    if (p->M == 0 || N == 0) return TCA_OK;
+    const size_t c_elem = c_dtype == TCA_DTYPE_F16 ? 2 : 4;
+    if (N % 8 != 0 || !aligned16(d_C) || ((size_t)ldc * c_elem) % 16 != 0)
+        return set_error(TCA_ERR_UNSUPPORTED,
+                         "the E4M3 forward needs N %% 8 == 0 and a 16-byte aligned C with 16-byte aligned rows");
+    if (p->K == 0)
+        return set_error(TCA_ERR_UNSUPPORTED, "K == 0: use tca_spmm (nothing to quantize)");
+    if (!p->has_fp8)
+        return set_error(TCA_ERR_INVALID_ARG,
+                         "the plan has no E4M3 form: call tca_plan_quantize_fp8 once first (it allocates)");
+    const int ldq = (N + 15) & ~15;
+    const size_t bq = ((size_t)p->K * ldq + 255) & ~(size_t)255;
+    const size_t need = bq + sizeof(float) * (size_t)ldq;
+    if (need > (size_t)TCA_FP8_STATIC_SCRATCH_BYTES)
+        return set_error(TCA_ERR_INVALID_ARG,
+                         "B of %d x %d needs %zu bytes of E4M3 scratch; the static scratch holds %u "
+                         "(K * round_up(N, 16) + 4 * round_up(N, 16) bytes must fit): use tca_spmm_fp8",
+                         p->K, N, need, (unsigned)TCA_FP8_STATIC_SCRATCH_BYTES);
+    void *base = nullptr;
+    TCA_TRY(static_scratch(&base));
+    cudaStream_t s = (cudaStream_t)stream;
+    uint8_t *Bq = static_cast<uint8_t *>(base);
+    float *scale = reinterpret_cast<float *>(static_cast<uint8_t *>(base) + bq);
+    TCA_TRY(quantize_b((const __half *)d_B_f16, ldb, p->K, N, Bq, ldq, scale, s));
+    SpmmJob job;
+    job.p = p;
+    job.B = (const __half *)d_B_f16;
+    job.C = d_C;
+    job.ldb = ldb;
+    job.N = N;
+    job.ldc = ldc;
+    job.f8 = true;
+    job.tc = p->n_tc > 0;
+    job.n_tile = pick_tc_tile(p->n_tc, N, false, true);
+    job.Bq = Bq;
+    job.ldq = ldq;
+    job.col_scale = scale;
+    // launched directly (no deferred launch list): nothing on this path allocates
+    TCA_TRY(launch_tc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
+    return launch_cc_jobs(&job, 1, c_dtype, alpha, beta, flags, s);
 }

@@ -96,6 +96,7 @@ _SIGS = {
     "tca_plan_quantize_fp8": ([_VP, _VP], _I),
     "tca_quantize_b_fp8": ([_P, _I, _I, _I, _P, _I, _P, _VP], _I),
     "tca_spmm_fp8": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP], _I),
+    "tca_spmm_fp8_static": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP], _I),
     "tca_spmm_fp8_batched": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _VP, ctypes.POINTER(_VP)], _I),
     "tca_batch_graph_create": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _I, ctypes.POINTER(_VP)], _I),
     "tca_batch_graph_launch": ([_VP, _VP], _I),
