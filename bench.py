@@ -215,8 +215,13 @@ def run_ours(args, world, rank):
     n_cc_jobs = sum(1 for p in plans if p.info()["n_cc_windows"] > 0)
     launches_per_step = -(-n_tc_jobs // 32) + -(-n_cc_jobs // 32)
 
+    # the step replays the batch captured as a CUDA graph (tca_batch_graph_*):
+    # the host side of an eager 32-problem call (argument checks, 64 TMA
+    # descriptors) costs more than its device time
+    graph16 = tca_spmm.BatchGraph(plans, Bs, Cs)
+
     def step():
-        tca_spmm.spmm_batched(plans, Bs, Cs)
+        graph16.launch()
 
     for _ in range(args.warmup):
         step()
@@ -270,8 +275,10 @@ def run_ours(args, world, rank):
 
     # FP8-E4M3 forward of the same step (per-row A / per-column B scales; B is
     # quantized inside every step), and the error of both precisions vs FP64
+    graph8 = tca_spmm.BatchGraph(plans, Bs, Cs, precision="e4m3")
+
     def step8():
-        tca_spmm.spmm_fp8_batched(plans, Bs, Cs)
+        graph8.launch()
 
     for _ in range(args.warmup):
         step8()
@@ -353,10 +360,58 @@ def run_ours(args, world, rank):
                                     "spmm_cc_stream_kernel": round(cc_mean * 1e3, 3)}},
         "e2e": e2e,
         "fp8": fp8,
+        "batching": batching_leg(args, world),
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
     }
     return out, distinct
+
+
+def batching_leg(args, world):
+    """The batching config: 24 layers of mixed shapes, sparsity and N, as one
+    autotuned batch replayed from a CUDA graph vs 24 sequential forwards
+    (tca_spmm per layer), device time per pass (CUDA events, median of runs)."""
+    import torch
+    import tca_spmm
+    from tca_spmm import gen
+    dev = torch.device("cuda", torch.cuda.current_device())
+    ls = gen.batch_layers()
+    plans, Bs, outs = [], [], []
+    for c in ls:
+        rp, ci, v = (torch.from_numpy(x.copy()).to(dev) for x in (c["row_ptr"], c["col"], c["vals"]))
+        plans.append(tca_spmm.Plan(rp, ci, v, c["K"]))
+        Bs.append(torch.from_numpy(c["B"].copy()).to(dev))
+        outs.append(torch.empty((c["M"], c["N"]), dtype=torch.float16, device=dev))
+    flops = sum(2.0 * c["col"].size * c["N"] for c in ls)
+    tuned = tca_spmm.autotune(plans, Bs, outs, reps=3)
+    g = tca_spmm.BatchGraph(plans, Bs, outs, n_tiles=[t[0] for t in tuned], cc_cols=[t[1] for t in tuned])
+
+    def seq():
+        for p, B, C in zip(plans, Bs, outs):
+            p.spmm(B, out=C)
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b) * 1e3)
+        return float(np.median(ts))
+
+    t_graph = timed(g.launch)
+    t_seq = timed(seq)
+    g.close()
+    return {"workload": "24 layers: 6 each of 512x2048, 2048x512, 512x512, 1024x4096; sparsity U[0.5, 0.98]; "
+                        "N per layer from {64..1024}; FP16",
+            "graph_us": round(t_graph, 2), "sequential_us": round(t_seq, 2),
+            "speedup": round(t_seq / t_graph, 3), "graph_gflops": round(flops / (t_graph * 1e-6) / 1e9, 1),
+            "tuned": [list(t) for t in tuned]}
 
 
 def run_reference(args, world, rank):
