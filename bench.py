@@ -238,19 +238,11 @@ def run_ours(args, world, rank):
     ms_step = ms_total / args.steps
     value = world * flops_step / (ms_step * 1e-3) / 1e9
 
-    # per-kernel device time: a second pass over the same steps with CUDA
-    # events recorded around the tensor-core and the CUDA-core launches
+    # per-kernel device time: the same batch captured once more with CUDA
+    # events recorded inside the graph around the tensor-core and the
+    # CUDA-core launches, replayed n_prof times
     n_prof = max(1, min(args.steps, 20))
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(n_prof)]
-    for e4 in evs:
-        for e in e4:
-            e.record()
-    torch.cuda.synchronize()
-    for k in range(n_prof):
-        tca_spmm.spmm_batched(plans, Bs, Cs, events=evs[k])
-    torch.cuda.synchronize()
-    tc_ms = [e[0].elapsed_time(e[1]) for e in evs]
-    cc_ms = [e[2].elapsed_time(e[3]) for e in evs]
+    tc_ms, cc_ms = kernel_times(tca_spmm, torch, plans, Bs, Cs, "f16", n_prof)
     # algorithmic bytes per launch, per problem part: the part's nonzeros
     # (2 B value + 4 B index), row offsets and output rows, plus B once
     tc_bytes = cc_bytes = 0
@@ -289,19 +281,11 @@ def run_ours(args, world, rank):
     e1.record()
     barrier(world)
     ms8 = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
-    evs8 = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(n_prof)]
-    for e4 in evs8:  # torch only reads events it has recorded itself once
-        for e in e4:
-            e.record()
-    torch.cuda.synchronize()
-    for k in range(n_prof):
-        tca_spmm.spmm_fp8_batched(plans, Bs, Cs, events=evs8[k])
-    torch.cuda.synchronize()
+    tc8_ms, cc8_ms = kernel_times(tca_spmm, torch, plans, Bs, Cs, "e4m3", n_prof)
     fp8 = {"value": round(world * flops_step / (ms8 * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
            "ms_per_step": round(ms8, 5), "speedup_vs_fp16": round(ms_step / ms8, 3),
-           "kernels_us": {"spmm_tc_kernel_e4m3": round(float(np.mean([e[0].elapsed_time(e[1]) for e in evs8])) * 1e3, 3),
-                          "spmm_cc_stream_kernel_e4m3":
-                              round(float(np.mean([e[2].elapsed_time(e[3]) for e in evs8])) * 1e3, 3)},
+           "kernels_us": {"spmm_tc_kernel_e4m3": round(float(np.mean(tc8_ms)) * 1e3, 3),
+                          "spmm_cc_stream_kernel_e4m3": round(float(np.mean(cc8_ms)) * 1e3, 3)},
            "quantization": "E4M3, per-row A and per-column B FP32 scales, FP32 accumulation, FP16 out; "
                            "B is quantized inside every step"}
     if rank == 0 and not args.no_cpu:
@@ -365,6 +349,24 @@ def run_ours(args, world, rank):
         "clocks": clk.summary(),
     }
     return out, distinct
+
+
+def kernel_times(tca_spmm, torch, plans, Bs, Cs, precision, reps):
+    """(tensor-core ms, CUDA-core ms) per replay of the batch captured in a
+    CUDA graph with events around each kernel group."""
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for e in ev:  # torch reads only events it has recorded itself once
+        e.record()
+    torch.cuda.synchronize()
+    g = tca_spmm.BatchGraph(plans, Bs, Cs, precision=precision, events=ev)
+    tc, cc = [], []
+    for _ in range(reps):
+        g.launch()
+        torch.cuda.synchronize()
+        tc.append(ev[0].elapsed_time(ev[1]))
+        cc.append(ev[2].elapsed_time(ev[3]))
+    g.close()
+    return tc, cc
 
 
 def batching_leg(args, world):

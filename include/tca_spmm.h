@@ -259,6 +259,13 @@ typedef struct tca_graph *tca_graph_t;
  * freeing any of them is undefined. */
 TCA_API int tca_batch_graph_create(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
                                    unsigned flags, int precision, tca_graph_t *graph);
+/* tca_batch_graph_create that also captures four caller-created CUDA events
+ * (cudaEvent_t, NULL entries skipped) into the graph, recorded around the
+ * tensor-core and the CUDA-core launches of every replay: per-kernel device
+ * time of the batch as it runs from the graph. */
+TCA_API int tca_batch_graph_create_events(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha,
+                                          float beta, unsigned flags, int precision, void *const *events,
+                                          tca_graph_t *graph);
 /* One replay of the captured batch on `stream`. */
 TCA_API int tca_batch_graph_launch(tca_graph_t graph, tca_stream_t stream);
 TCA_API int tca_batch_graph_destroy(tca_graph_t graph);

@@ -26,11 +26,11 @@ namespace tca {
 namespace {
 
 int run_batch(const tca_batch_item_t *items, int n, int c_dtype, float alpha, float beta, unsigned flags, int precision,
-              cudaStream_t s)
+              cudaStream_t s, void *const *events = nullptr)
 {
     return precision == TCA_PRECISION_E4M3
-               ? tca_spmm_fp8_batched(items, n, c_dtype, alpha, beta, flags, s, nullptr)
-               : tca_spmm_batched(items, n, c_dtype, alpha, beta, flags, s, nullptr);
+               ? tca_spmm_fp8_batched(items, n, c_dtype, alpha, beta, flags, s, events)
+               : tca_spmm_batched(items, n, c_dtype, alpha, beta, flags, s, events);
 }
 
 struct StreamGuard {
@@ -46,6 +46,12 @@ using namespace tca;
 int tca_batch_graph_create(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
                            unsigned flags, int precision, tca_graph_t *out)
 {
+    return tca_batch_graph_create_events(items, n_items, c_dtype, alpha, beta, flags, precision, nullptr, out);
+}
+
+int tca_batch_graph_create_events(const tca_batch_item_t *items, int n_items, int c_dtype, float alpha, float beta,
+                                  unsigned flags, int precision, void *const *events, tca_graph_t *out)
+{
     clear_error();
     if (!out) return set_error(TCA_ERR_INVALID_ARG, "graph output pointer is NULL");
     *out = nullptr;
@@ -60,7 +66,7 @@ int tca_batch_graph_create(const tca_batch_item_t *items, int n_items, int c_dty
     TCA_CUDA_TRY(cudaStreamSynchronize(g.s));
     cudaGraph_t graph = nullptr;
     TCA_CUDA_TRY(cudaStreamBeginCapture(g.s, cudaStreamCaptureModeRelaxed));
-    const int st = run_batch(items, n_items, c_dtype, alpha, beta, flags, precision, g.s);
+    const int st = run_batch(items, n_items, c_dtype, alpha, beta, flags, precision, g.s, events);
     const cudaError_t ce = cudaStreamEndCapture(g.s, &graph);
     if (st != TCA_OK) {
         if (graph) cudaGraphDestroy(graph);

@@ -91,42 +91,81 @@ __global__ void k_col_zero(const __grid_constant__ QBatch b)
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < q.N; n += gridDim.x * blockDim.x) q.colmax[n] = 0u;
 }
 
+// B rows load 8 halves (16 bytes) at a time when B and its rows are 16-byte
+// aligned; otherwise one half at a time.
+__device__ __forceinline__ bool vec8_ok(const QJob &q)
+{
+    return (reinterpret_cast<uintptr_t>(q.B) & 15u) == 0 && (q.ldb & 7) == 0;
+}
+
+__device__ __forceinline__ void load8h(const QJob &q, int k, int n, bool vec, float *v)
+{
+    const __half *row = q.B + (size_t)k * q.ldb;
+    if (vec && n + 8 <= q.N) {
+        const uint4 u = __ldg(reinterpret_cast<const uint4 *>(row + n));
+        const __half2 *h = reinterpret_cast<const __half2 *>(&u);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float2 f = __half22float2(h[i]);
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = n + i < q.N ? __half2float(row[n + i]) : 0.f;
+    }
+}
+
 // Column absolute maxima (FP32 bit patterns order like the non-negative
-// values): thread = column, blockIdx.y = 32 rows of B.
+// values): thread = 8 consecutive columns, blockIdx.y = 32 rows of B.
 __global__ void k_col_absmax(const __grid_constant__ QBatch b)
 {
     const QJob &q = b.job[blockIdx.z];
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
     const int k0 = blockIdx.y * 32;
     if (n >= q.N || k0 >= q.K)
         return;
+    const bool vec = vec8_ok(q);
     const int k1 = min(q.K, k0 + 32);
-    float m = 0.f;
-    for (int k = k0; k < k1; k++) m = fmaxf(m, fabsf(__half2float(q.B[(size_t)k * q.ldb + n])));
-    atomicMax(q.colmax + n, __float_as_uint(m));
+    float m[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int k = k0; k < k1; k++) {
+        float v[8];
+        load8h(q, k, n, vec, v);
+#pragma unroll
+        for (int i = 0; i < 8; i++) m[i] = fmaxf(m[i], fabsf(v[i]));
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        if (n + i < q.N)
+            atomicMax(q.colmax + n + i, __float_as_uint(m[i]));
 }
 
-// Bq[k, n] = E4M3(B[k, n] / s[n]); thread = 4 consecutive columns, rows blockIdx.y, + gridDim.y, ...
+// Bq[k, n] = E4M3(B[k, n] / s[n]); thread = 8 consecutive columns, rows
+// blockIdx.y, + gridDim.y, ...
 __global__ void k_quant_cols(const __grid_constant__ QBatch b)
 {
     const QJob &q = b.job[blockIdx.z];
-    const int n = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int n = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
     if (n >= q.N)
         return;
-    float s[4];
+    const bool vec = vec8_ok(q);
+    float s[8];
 #pragma unroll
-    for (int i = 0; i < 4; i++) s[i] = n + i < q.N ? scale_of(__uint_as_float(q.colmax[n + i])) : 1.f;
+    for (int i = 0; i < 8; i++) s[i] = n + i < q.N ? scale_of(__uint_as_float(q.colmax[n + i])) : 1.f;
     for (int k = blockIdx.y; k < q.K; k += gridDim.y) {
-        uint32_t packed = 0;
+        float v[8];
+        load8h(q, k, n, vec, v);
+        uint32_t lo = 0, hi = 0;
 #pragma unroll
-        for (int i = 0; i < 4; i++)
-            if (n + i < q.N)
-                packed |= (uint32_t)to_e4m3(__half2float(q.B[(size_t)k * q.ldb + n + i]) / s[i]) << (8 * i);
+        for (int i = 0; i < 4; i++) {
+            lo |= (uint32_t)to_e4m3(v[i] / s[i]) << (8 * i);
+            hi |= (uint32_t)to_e4m3(v[4 + i] / s[4 + i]) << (8 * i);
+        }
         uint8_t *dst = q.Bq + (size_t)k * q.ldq + n;
-        if (n + 4 <= q.N) {
-            *reinterpret_cast<uint32_t *>(dst) = packed;
+        if (n + 8 <= q.N && (reinterpret_cast<uintptr_t>(dst) & 7u) == 0) {
+            *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
         } else {
-            for (int i = 0; n + i < q.N; i++) dst[i] = (uint8_t)(packed >> (8 * i));
+            for (int i = 0; n + i < q.N && i < 8; i++) dst[i] = (uint8_t)((i < 4 ? lo : hi) >> (8 * (i & 3)));
         }
     }
 }
@@ -152,8 +191,8 @@ int quantize_b_batch(const QBatch &b, cudaStream_t s)
         return TCA_OK;
     const unsigned z = (unsigned)b.n;
     k_col_zero<<<dim3(blocks(maxN, 256), 1, z), 256, 0, s>>>(b);
-    k_col_absmax<<<dim3(blocks(maxN, 256), blocks(maxK, 32), z), 256, 0, s>>>(b);
-    k_quant_cols<<<dim3(blocks(blocks(maxN, 4), 128), (unsigned)std::min(maxK, 65535), z), 128, 0, s>>>(b);
+    k_col_absmax<<<dim3(blocks(blocks(maxN, 8), 128), blocks(maxK, 32), z), 128, 0, s>>>(b);
+    k_quant_cols<<<dim3(blocks(blocks(maxN, 8), 128), (unsigned)std::min(blocks(maxK, 8), 65535u), z), 128, 0, s>>>(b);
     k_col_scale<<<dim3(blocks(maxN, 256), 1, z), 256, 0, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;

@@ -658,8 +658,14 @@ int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alp
     LaunchList tc, cc;
     TCA_TRY(launch_tc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &tc));
     TCA_TRY(launch_cc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &cc));
+    // Under stream capture a plain record only orders the graph; an external
+    // record becomes a graph node that records the event at every replay.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (events)
+        TCA_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
+    const unsigned rec_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
     auto rec = [&](int i) -> int {
-        if (events && events[i]) TCA_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[i], s));
+        if (events && events[i]) TCA_CUDA_TRY(cudaEventRecordWithFlags((cudaEvent_t)events[i], s, rec_flags));
         return TCA_OK;
     };
     TCA_TRY(rec(0));

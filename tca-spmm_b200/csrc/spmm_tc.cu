@@ -21,8 +21,9 @@
 //     pre-swizzled dense A tile (chunks with >= 2048 nonzeros: one 16 KB
 //     cp.async.bulk) or its packed entries (cp.async.bulk into the stage's
 //     staging buffer);
-//   * scatter warps, once a stage's entries landed, zero its A tile and
-//     scatter them into the 128-byte swizzled K-major layout;
+//   * scatter warps (two groups taking chunks in turn), once a stage's
+//     entries landed, zero its A tile and scatter them into the swizzled
+//     K-major layout;
 //   * one MMA lane issues 4 tcgen05.mma (K = 16 each) per chunk into the FP32
 //     accumulator in tensor memory and releases the stage with tcgen05.commit;
 //   * finally 4 warps read the accumulator (TMEM lane = row) and store
@@ -140,7 +141,7 @@ __device__ __forceinline__ void store8_out(float *p, const float *v, float alpha
 
 // Shared memory (1024-byte aligned base): kStages x (A tile | B tile),
 // kStages entry staging buffers, per-stage chunk records, the CTA's item
-// table, mbarriers and two broadcast flags + TMEM slot.
+// table, mbarriers, four broadcast flags and the TMEM slot.
 // F8: E4M3 operands -- an 8 KB A tile (64-byte swizzled K-major) and 64 x NT
 // byte B tiles, so the ring holds more stages.
 template <int NT, bool F8> struct TcCfg {
@@ -155,8 +156,8 @@ template <int NT, bool F8> struct TcCfg {
     static constexpr int kPend2Off = kPendOff + kStages * 16;              // int4 [kStages]: flags, buffer, item
     static constexpr int kItemOff = kPend2Off + kStages * 16;              // int4 [kMaxCtaItems]
     static constexpr int kBarOff = kItemOff + kMaxCtaItems * 16;
-    // full, empty, staged [kStages]; accum_full, accum_empty [2]
-    static constexpr int kSmem = kBarOff + (3 * kStages + 4) * 8 + 16;
+    // full, empty, staged [kStages]; accum_full, accum_empty [2]; 4 flags, TMEM slot
+    static constexpr int kSmem = kBarOff + (3 * kStages + 4) * 8 + 24;
     static_assert(kSmem <= 227 * 1024, "shared memory budget");
     static_assert(kStage % 1024 == 0 && kATileBytes % 1024 == 0, "swizzled tiles need 1024-byte alignment");
     static_assert(kStagingOff % 16 == 0 && kStagingBytes % 16 == 0 && kPendOff % 16 == 0, "16-byte alignment");
@@ -177,27 +178,31 @@ __device__ __forceinline__ int4 decode_item(const TcBatch &batch, int item)
 }
 
 // Persistent CTAs, one per SM: CTA b processes work items b, b + gridDim.x,
-// ... (at most kMaxCtaItems), as one continuous stream of chunks through the
-// stage ring. Warp roles (kThreads threads):
+// ... (at most kMaxCtaItems), as one continuous stream of total_chunks chunks
+// through the stage ring; every role runs over exactly those chunks. Roles
+// (kThreads threads):
 //   warps 4, 10, 11, 12 (loaders; loader l takes chunks g = l (mod kLoaders),
 //     so that four chunks are being issued at once -- one warp issuing every
 //     chunk in turn was measured to need ~0.9 us per chunk, three times the
-//     tensor-core time of an N = 256 chunk): per chunk, acquire the stage ("empty"), write the
-//     chunk's records (entries range and image for the scatter warps; first /
-//     last chunk of its item and accumulator buffer for the MMA lane), set the
-//     "full" transaction count and issue the dense A image (16 KB
-//     cp.async.bulk) or the sparse entries (cp.async.bulk into staging,
+//     tensor-core time of an N = 256 chunk): per chunk, acquire the stage
+//     ("empty"), write the chunk's records (entries range and image for the
+//     scatter warps; first / last chunk of its item and accumulator buffer for
+//     the MMA lane), set the "full" transaction count and issue the dense A
+//     image (cp.async.bulk) or the sparse entries (cp.async.bulk into staging,
 //     completing on "staged"), then the B rows: tiled TMA boxes of 64
 //     contiguous rows for direct chunks, tile::gather4 for condensed ones.
 //     Chunk metadata (columns, image, entry range) is loaded into registers
-//     one chunk of the same loader ahead. The loader owning position
-//     total_chunks passes an end record through the ring.
-//   warps 0-3 (scatter): per chunk, wait "staged"; for a sparse chunk zero the
-//     A tile, scatter the staged entries, fence.proxy.async; arrive "full".
+//     one chunk of the same loader ahead.
+//   warps 0-3 (scatter; two groups of two warps taking chunks in turn when
+//     the ring has an even number of stages, else one group of four): per
+//     chunk, wait "staged"; for a sparse chunk zero the A tile, scatter the
+//     staged entries, fence.proxy.async; arrive "full". With two groups, a
+//     group's previous use of a stage is its own (stage count even), so no
+//     group waits on a phase more than one ahead of an mbarrier.
 //   warp 5, lane 0 (MMA): per chunk wait "full"; on an item's first chunk
 //     wait until its TMEM accumulator buffer (item parity) is drained
-//     ("accum_empty"); 4 x tcgen05.mma; commit "empty"; on the item's last
-//     chunk commit "accum_full".
+//     ("accum_empty"); 4 x tcgen05.mma (2 for E4M3); commit "empty"; on the
+//     item's last chunk commit "accum_full".
 //   warps 6-9 (epilogue): per item wait "accum_full", tcgen05.ld the rows
 //     (warp w reads TMEM lanes 32 (w % 4) ..), alpha/beta, store to C[perm],
 //     arrive "accum_empty" -- overlapping the next item's main loop.
@@ -218,8 +223,10 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     uint64_t *staged = empty + S;
     uint64_t *acc_full = staged + S;  // [2]
     uint64_t *acc_empty = acc_full + 2; // [2]
-    volatile int *flag = reinterpret_cast<volatile int *>(acc_empty + 2); // 2 slots, alternating by chunk
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + 2) + 2;
+    volatile int *flag = reinterpret_cast<volatile int *>(acc_empty + 2); // 2 slots per scatter group
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + 2) + 4;
+    constexpr int kScatterGroups = S % 2 == 0 ? 2 : 1; // two groups need an even ring (see the scatter role)
+    constexpr int kGroupThreads = kScatterThreads / kScatterGroups;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = batch.item_start[batch.n_jobs];
@@ -231,7 +238,7 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     }
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; s++) {
-            mbar_init(&full[s], kScatterThreads);
+            mbar_init(&full[s], kGroupThreads);
             mbar_init(&empty[s], 1);
             mbar_init(&staged[s], 1);
         }
@@ -254,14 +261,14 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
+    int total_chunks = 0; // of this CTA's items: every role runs over exactly these
+    for (int k = 0; k < n_items; k++) total_chunks += items[k].z;
 
     if (warp == kLoaderWarp || warp >= kLoaderWarp1) {
         // ---------------- loaders ----------------
         // Loader ld issues chunks g = ld, ld + kLoaders, ... of the CTA's chunk
         // stream; (k, i) is the item and chunk-within-item of its next chunk.
         const int ld = warp == kLoaderWarp ? 0 : warp - kLoaderWarp1 + 1;
-        int total_chunks = 0;
-        for (int k = 0; k < n_items; k++) total_chunks += items[k].z;
         auto advance = [&](int &k, int &i) {
             while (k < n_items && i >= items[k].z) { i -= items[k].z; k++; }
         };
@@ -285,19 +292,23 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         };
         int k = 0, i = ld;
         advance(k, i);
-        Meta cur, nxt;
-        fetch(k, i, cur);
         int g = ld;
-        for (; g < total_chunks; g += kLoaders) {
+        // One chunk: prefetch the metadata of this loader's next chunk into
+        // `nxt`, acquire the stage, issue the chunk described by `cur`. The
+        // loop below alternates the roles of two Meta variables (unrolled by
+        // two), so that no register copy waits for a prefetch still in flight.
+        auto step = [&](Meta &cur, Meta &nxt) -> bool {
+            if (g >= total_chunks || !ok)
+                return false;
             int k2 = k, i2 = i + kLoaders;
             advance(k2, i2);
-            fetch(k2, i2, nxt); // in flight while this chunk's stage is acquired and issued
+            fetch(k2, i2, nxt);
             const int s = g % S;
             uint32_t got = 1;
             if (lane == 0 && g >= S)
                 got = mbar_wait(&empty[s], ((g / S) - 1) & 1) ? 1u : 0u;
             got = __shfl_sync(0xffffffffu, got, 0);
-            if (!got) { ok = false; break; }
+            if (!got) { ok = false; return false; }
             const int4 it = items[k];
             const TcJob &a = batch.job[it.w >> 16];
             const int n0 = (it.w & 0xffff) * NT;
@@ -323,7 +334,7 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             const int col0 = __shfl_sync(0xffffffffu, cur.cols.x, 0);
             const int col63 = __shfl_sync(0xffffffffu, cur.cols.w, 15);
             if (col0 >= 0 && col63 == col0 + kChunkCols - 1) {
-                // 64 contiguous B rows (direct chunks): one 8 KB tiled box per 64 columns
+                // 64 contiguous B rows (direct chunks): one 8 KB tiled box per 128-byte column slab
                 if (lane < kBoxes)
                     tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * Cfg::kBoxCols, col0,
                                &full[s]);
@@ -337,69 +348,60 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                 for (int q = lane; q < kGathers; q += 32) {
                     const int box = q >> 4;
                     tma_gather4(b_s + box * (kChunkCols * 128) + src * 512, &a.tmap_b, n0 + box * Cfg::kBoxCols, y0,
-                                y1, y2, y3,
-                                &full[s]);
+                                y1, y2, y3, &full[s]);
                 }
             }
-            cur = nxt;
             k = k2;
             i = i2;
-        }
-        // end record (written by the loader that owns chunk position total_chunks):
-        // the scatter warps and the MMA lane stop at it
-        if (ok && g == total_chunks) {
-            const int s = g % S;
-            uint32_t got = 1;
-            if (lane == 0 && g >= S)
-                got = mbar_wait(&empty[s], ((g / S) - 1) & 1) ? 1u : 0u;
-            got = __shfl_sync(0xffffffffu, got, 0);
-            if (got && lane == 0) {
-                pend[s] = make_int4(-2, 0, 0, 0);
-                mbar_arrive(&staged[s]);
-            }
-            if (!got) ok = false;
+            g += kLoaders;
+            return true;
+        };
+        Meta ma, mb;
+        fetch(k, i, ma);
+        while (step(ma, mb) && step(mb, ma)) {
         }
     } else if (warp < 4) {
         // ---------------- scatter ----------------
-        const int sid = threadIdx.x;
-        for (int g = 0;; g++) {
+        // kScatterGroups groups of warps take the chunks in turn (group q:
+        // chunks g = q (mod kScatterGroups)), so that the scatter of one sparse
+        // chunk overlaps the next one's.
+        const int grp = kScatterGroups == 2 ? (warp >> 1) : 0;
+        const int sid = (int)threadIdx.x - grp * kGroupThreads;
+        int it = 0;
+        for (int g = grp; g < total_chunks; g += kScatterGroups, it++) {
             const int s = g % S;
+            volatile int *fl = flag + grp * 2 + (it & 1);
             if (sid == 0)
-                flag[g & 1] = mbar_wait(&staged[s], (g / S) & 1) ? 1 : 0;
-            named_bar_sync(1, kScatterThreads); // also orders the staged data for every scatter thread
-            if (flag[g & 1] == 0) { ok = false; break; } // uniform across the scatter warps
+                *fl = mbar_wait(&staged[s], (g / S) & 1) ? 1 : 0;
+            named_bar_sync(1 + grp, kGroupThreads); // also orders the staged data for every thread of the group
+            if (*fl == 0) { ok = false; break; } // uniform across the group
             const int4 pd = pend[s];
-            if (pd.x >= -1 && pd.x < 0) {
+            if (pd.x == -1) {
                 uint8_t *At = smem + s * Cfg::kStage;
 #pragma unroll
-                for (int k = 0; k < kATileBytes / (16 * kScatterThreads); k++)
-                    reinterpret_cast<uint4 *>(At)[sid + k * kScatterThreads] = make_uint4(0, 0, 0, 0);
-                named_bar_sync(1, kScatterThreads);
+                for (int q = 0; q < kATileBytes / (16 * kGroupThreads); q++)
+                    reinterpret_cast<uint4 *>(At)[sid + q * kGroupThreads] = make_uint4(0, 0, 0, 0);
+                named_bar_sync(1 + grp, kGroupThreads);
                 const uint32_t *st = reinterpret_cast<const uint32_t *>(smem + Cfg::kStagingOff + s * kStagingBytes);
-                for (int e = pd.y + sid; e < pd.w; e += kScatterThreads) {
+                for (int e = pd.y + sid; e < pd.w; e += kGroupThreads) {
                     const uint32_t v = st[e - pd.z];
                     if constexpr (F8)
                         At[swz64_offset(v >> 22, (v >> 16) & 63u)] = (uint8_t)(v & 0xffu);
                     else
                         *reinterpret_cast<uint16_t *>(At + swz128_offset(v >> 22, (v >> 16) & 63u)) =
-                        (uint16_t)(v & 0xffffu);
+                            (uint16_t)(v & 0xffffu);
                 }
                 fence_proxy_async();
             }
             mbar_arrive(&full[s]);
-            if (pd.x == -2)
-                break; // end record
         }
     } else if (warp == kMmaWarp) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_f16(NT); // E4M3 has format code 0 in kind::f8f6f4 as FP16 in kind::f16
-            for (int g = 0;; g++) {
+            for (int g = 0; g < total_chunks; g++) {
                 const int s = g % S;
                 if (!mbar_wait(&full[s], (g / S) & 1)) { ok = false; break; }
-                const int4 pd = pend[s];
-                if (pd.x == -2)
-                    break; // end record
                 const int4 f = pend2[s];
                 const int b = f.y, k = f.z;
                 if ((f.x & 1) && k >= 2 && !mbar_wait(&acc_empty[b], ((k >> 1) - 1) & 1)) { ok = false; break; }
@@ -457,10 +459,20 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                     break; // uniform across the warp
                 uint32_t r[16];
                 tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * NT + cb * 16), r);
-                if constexpr (F8) { // dequantise: row scale x column scale
+                if constexpr (F8) { // dequantise: row scale x column scale (16-byte aligned scale vectors)
                     float *f = reinterpret_cast<float *>(r);
+                    const float4 *cs = reinterpret_cast<const float4 *>(a.col_scale + n);
+                    float sb[16];
 #pragma unroll
-                    for (int q = 0; q < 16; q++) f[q] *= sa * __ldg(a.col_scale + min(n + q, a.N - 1));
+                    for (int q = 0; q < 4; q++) {
+                        const float4 v = (n + 4 * q < a.N) ? __ldg(cs + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+                        sb[4 * q] = v.x;
+                        sb[4 * q + 1] = v.y;
+                        sb[4 * q + 2] = v.z;
+                        sb[4 * q + 3] = v.w;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 16; q++) f[q] *= sa * sb[q];
                 }
                 if (Crow) {
                     store8_out(Crow + n, reinterpret_cast<const float *>(r), a.alpha, a.beta);

@@ -99,6 +99,8 @@ _SIGS = {
     "tca_spmm_fp8_static": ([_VP, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP], _I),
     "tca_spmm_fp8_batched": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _VP, ctypes.POINTER(_VP)], _I),
     "tca_batch_graph_create": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _I, ctypes.POINTER(_VP)], _I),
+    "tca_batch_graph_create_events": ([ctypes.POINTER(BatchItem), _I, _I, _F, _F, _U, _I, ctypes.POINTER(_VP),
+                                       ctypes.POINTER(_VP)], _I),
     "tca_batch_graph_launch": ([_VP, _VP], _I),
     "tca_batch_graph_destroy": ([_VP], _I),
     "tca_batch_autotune": ([ctypes.POINTER(BatchItem), _I, _I, _I, _I, _VP], _I),
@@ -403,15 +405,22 @@ class BatchGraph:
     the plans and tensors, whose addresses the graph keeps."""
 
     def __init__(self, plans, Bs, outs, alpha=1.0, beta=0.0, keep_empty_rows=False, precision="f16",
-                 n_tiles=None, cc_cols=None):
-        self._keep = (list(plans), list(Bs), list(outs))
+                 n_tiles=None, cc_cols=None, events=None):
+        """events: 4 torch.cuda.Event (or None) recorded inside the graph around
+        the tensor-core and the CUDA-core launches of every replay."""
+        self._keep = (list(plans), list(Bs), list(outs), events)
         self._lib = lib()
         arr = _batch_items(plans, Bs, outs, n_tiles, cc_cols)
         code = _out_code(outs[0].dtype) if plans else DTYPE_F16
         flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
         h = _VP()
-        _check(self._lib.tca_batch_graph_create(arr, len(plans), code, alpha, beta, flags, _PRECISIONS[precision],
-                                                ctypes.byref(h)))
+        if events is None:
+            _check(self._lib.tca_batch_graph_create(arr, len(plans), code, alpha, beta, flags,
+                                                    _PRECISIONS[precision], ctypes.byref(h)))
+        else:
+            ev = (_VP * 4)(*[(e.cuda_event if e is not None else None) for e in events])
+            _check(self._lib.tca_batch_graph_create_events(arr, len(plans), code, alpha, beta, flags,
+                                                           _PRECISIONS[precision], ev, ctypes.byref(h)))
         self._h = h
 
     def launch(self, stream=None):
