@@ -72,6 +72,14 @@ TCA_API int tca_spmm_csr(const int *d_row_ptr, const int *d_col_idx, const void 
                  void *d_C, int ldc, int c_dtype,
                  float alpha, float beta, unsigned flags, tca_stream_t stream);
 
+/* FP64 forward, plan-free, on CUDA cores: C = alpha * A * B + beta * C with
+ * FP64 values, B and C and FP64 accumulation (TCA_FLAG_KEEP_EMPTY_ROWS as
+ * for tca_spmm_csr). The reference names an FP64 data type
+ * (src/arg_parse.h:102-105, src/general.cuh:58,65) but has no FP64 path. */
+TCA_API int tca_spmm_csr_f64(const int *d_row_ptr, const int *d_col_idx, const double *d_vals, int M, int K, int nnz,
+                             const double *d_B, int ldb, int N, double *d_C, int ldc, double alpha, double beta,
+                             unsigned flags, tca_stream_t stream);
+
 /* ------------------------------------------------------------------ */
 /* Plans: the row-window, column-condensed tile format.
  * tca_plan_create builds it on the GPU from a device CSR (replacing the
@@ -293,6 +301,20 @@ TCA_API int tca_smtx_parse(const char *text, size_t len, int *M, int *K, int *nn
                            int **row_ptr, int **col_idx, void **vals_f16);
 TCA_API int tca_smtx_read(const char *path, int *M, int *K, int *nnz,
                           int **row_ptr, int **col_idx, void **vals_f16);
+/* MatrixMarket coordinate text, read as the reference's mtx_input_to_CSR
+ * (src/file_input.cu:63-134): '%' lines are comments, the first other line
+ * is "rows cols nnz", each further line "r c [v]" (1-based unless
+ * zero_based). pattern_only: every value is 1.0 (a third token is ignored);
+ * otherwise a missing value is missing_value (the reference's CSR reader:
+ * 0.0; its dense reader, src/file_input.cu:8-62: 1.0). Rows come out in
+ * order with each row's entries in file order (no sorting; duplicates kept);
+ * values rounded to FP16. TCA_ERR_FORMAT for a count that differs from the
+ * header, an index out of range or a line that is not "r c [v]" (blank
+ * lines are skipped). Arrays are malloc'd; free with tca_free. */
+TCA_API int tca_mtx_parse(const char *text, size_t len, int zero_based, int pattern_only, float missing_value,
+                          int *M, int *K, int *nnz, int **row_ptr, int **col_idx, void **vals_f16);
+TCA_API int tca_mtx_read(const char *path, int zero_based, int pattern_only, float missing_value, int *M, int *K,
+                         int *nnz, int **row_ptr, int **col_idx, void **vals_f16);
 /* Writes the smtx layout (values line only when vals_f16 is not NULL). */
 TCA_API int tca_smtx_write(const char *path, int M, int K, int nnz, const int *row_ptr,
                            const int *col_idx, const void *vals_f16);

@@ -64,6 +64,13 @@ TCA_API void our_spmm_balanced(CSR *A_csr, half *B, float *C, int M, int N, int 
 TCA_API void perform_cuSPARSE_SpMM(half *A, half *B, float *C, int M, int N, int K, int num_iter,
                                    double *elapsed = NULL);
 
+/* src/spmm_cusparse.cuh:14, src/spmm_cusparse.cu:181 -- cuSPARSE Blocked-ELL
+ * SpMM comparator on a dense A cut into ell_block_size square blocks (block
+ * rows keep their occupied blocks, padded to the widest): FP16 A/B, FP32
+ * compute and C, ALG_DEFAULT, one untimed then num_iter timed calls. */
+TCA_API void perform_cuSPARSE_BlockSpMM(half *A, half *B, float *C, int M, int N, int K, int num_iter,
+                                        int ell_block_size, double *elapsed = NULL);
+
 /* src/gemm_cublas.cuh:12, src/gemm_cublas.cu:3 -- dense cuBLAS GemmEx gold:
  * FP16 A/B, FP32 C and compute, 5 warm-up then n_iter timed calls. */
 TCA_API void perform_GemmEx(half *A, half *B, float *C, int M, int N, int K, int n_iter,
@@ -80,6 +87,45 @@ TCA_API void smtx_input_to_Dense(std::ifstream &fin, half **mat, char *filename,
  * .smtx file straight into a malloc'd CSR (values 1.0 unless a values line is
  * present). `arg` is unused. */
 TCA_API void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, void *arg = NULL);
+
+/* src/general.cuh:54-59 */
+typedef enum entry_dtype { fp16, fp32, fp64 } entry_dtype;
+
+/* src/arg_parse.h:15-31 -- the reference's run options, layout-identical (the
+ * MatrixMarket readers take a pointer to it and read pattern_only and
+ * input_is_zero_based). The command-line parsing constructor of the reference
+ * is not provided (its CLI is outside this library); the default constructor
+ * sets the reference's defaults (src/general.cuh:21-28, src/arg_parse.h:33-48). */
+class TCA_API Arguments
+{
+public:
+    int M;
+    int N;
+    int K;
+    int num_iter;
+    bool pattern_only;
+    bool input_is_zero_based;
+    bool input_file_exists;
+    float target_sparsity;
+    float tolerance;
+    entry_dtype a_type, b_type, c_type;
+    char *input_fname;
+    int ell_block_size;
+    Arguments();
+};
+
+/* src/file_input.cuh:6-7, src/file_input.cu:8-134 -- MatrixMarket coordinate
+ * files ('%' comments, "rows cols nnz", then "r c [v]" lines, 1-based unless
+ * arg->input_is_zero_based) into a malloc'd CSR (rows grouped, file order
+ * within a row; missing values 0.0, or 1.0 with arg->pattern_only) or a
+ * malloc'd dense FP16 matrix (missing values 1.0, later duplicates win). A
+ * NULL arg means the defaults. Malformed text (count mismatch, indices out
+ * of range) is an error (see tca_mtx_parse) where the reference asserts or
+ * reads out of bounds. */
+TCA_API void mtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg);
+TCA_API void mtx_input_to_Dense(std::ifstream &fin, half **mat, Arguments *arg);
+/* src/file_input.cuh:9 with the reference's parameter type. */
+TCA_API void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg);
 
 /* src/general.cuh:135-138, src/miscalleneous.cu:29-112 */
 TCA_API void convert_dense_to_csr(half *mat, CSR **descr, int nRow, int nCol);

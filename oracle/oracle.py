@@ -61,6 +61,10 @@ def lib() -> ctypes.CDLL:
         L.orc_plan_build.argtypes = [_P, _P, _P, _I, _I, _I, _I, ctypes.c_float, _I, ctypes.POINTER(OrcPlan)]
         L.orc_plan_build.restype = _I
         L.orc_plan_free.argtypes = [ctypes.POINTER(OrcPlan)]; L.orc_plan_free.restype = None
+        L.orc_mtx_parse.argtypes = [ctypes.c_char_p, ctypes.c_long, _I, _I, ctypes.c_float, _P, _P,
+                                    ctypes.POINTER(ctypes.POINTER(_I)), ctypes.POINTER(ctypes.POINTER(_I)),
+                                    ctypes.POINTER(ctypes.POINTER(ctypes.c_uint16))]
+        L.orc_mtx_parse.restype = ctypes.c_long
         L.orc_f32_to_e4m3.argtypes = [ctypes.c_float]; L.orc_f32_to_e4m3.restype = ctypes.c_uint8
         L.orc_e4m3_to_f32.argtypes = [ctypes.c_uint8]; L.orc_e4m3_to_f32.restype = ctypes.c_float
         L.orc_quant_rows.argtypes = [_I, _P, _P, _P, _P]; L.orc_quant_rows.restype = None
@@ -205,6 +209,25 @@ def build_plan(row_ptr, col_idx, vals, K, sort_rows=True, tc_min_density=0.02, p
 
 
 # ---------------------------------------------------------------- reference library
+def mtx_parse(text: bytes, zero_based=True, pattern_only=False, missing=0.0):
+    """(M, K, row_ptr, col, vals fp16) of MatrixMarket text (orc_mtx_parse), or None if malformed."""
+    L = lib()
+    M, K = ctypes.c_int(), ctypes.c_int()
+    rp, ci = ctypes.POINTER(ctypes.c_int)(), ctypes.POINTER(ctypes.c_int)()
+    va = ctypes.POINTER(ctypes.c_uint16)()
+    n = L.orc_mtx_parse(text, len(text), int(zero_based), int(pattern_only), missing, ctypes.byref(M),
+                        ctypes.byref(K), ctypes.byref(rp), ctypes.byref(ci), ctypes.byref(va))
+    if n < 0:
+        return None
+    libc = ctypes.CDLL(None)
+    out = (M.value, K.value, np.ctypeslib.as_array(rp, (M.value + 1,)).copy(),
+           np.ctypeslib.as_array(ci, (max(n, 1),))[:n].copy(),
+           np.ctypeslib.as_array(va, (max(n, 1),))[:n].copy().view(np.float16))
+    for ptr in (rp, ci, va):
+        libc.free(ptr)
+    return out
+
+
 def e4m3_table() -> np.ndarray:
     """The FP32 value of every E4M3 code (orc_e4m3_to_f32); NaN codes are NaN."""
     L = lib()
@@ -276,10 +299,17 @@ def ref() -> ctypes.CDLL:
         R.ref_dense_to_csr.restype = _I
         R.ref_csr_to_dense.argtypes = [_I, _I, _I, _P, _P, _P, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint16))]
         R.ref_csr_to_dense.restype = _I
+        R.ref_mtx_to_csr.argtypes = [ctypes.c_char_p, _I, _I, _P, _P, _P, ctypes.POINTER(ctypes.POINTER(_I)),
+                                     ctypes.POINTER(ctypes.POINTER(_I)), ctypes.POINTER(ctypes.POINTER(ctypes.c_uint16))]
+        R.ref_mtx_to_csr.restype = ctypes.c_int
+        R.ref_mtx_to_dense.argtypes = [ctypes.c_char_p, _I, _P, _P, ctypes.POINTER(ctypes.POINTER(ctypes.c_uint16))]
+        R.ref_mtx_to_dense.restype = ctypes.c_int
         R.ref_naive_gemm.argtypes = [_P, _P, _P, _I, _I, _I]; R.ref_naive_gemm.restype = None
         R.ref_our_spmm_balanced.argtypes = [_I, _I, _I, _I, _P, _P, _P, _P, _P, _I, D]
         R.ref_our_spmm_balanced.restype = None
         R.ref_cusparse_spmm.argtypes = [_P, _P, _P, _I, _I, _I, _I, D]; R.ref_cusparse_spmm.restype = None
+        R.ref_cusparse_blockspmm.argtypes = [_P, _P, _P, _I, _I, _I, _I, _I, D]
+        R.ref_cusparse_blockspmm.restype = None
         R.ref_gemmex.argtypes = [_P, _P, _P, _I, _I, _I, _I, D]; R.ref_gemmex.restype = None
         _ref = R
     return _ref
@@ -310,6 +340,32 @@ def ref_dense_to_csr(A):
     ref().ref_dense_to_csr(Ab.ctypes.data, M, K, ctypes.byref(nnz), ctypes.byref(rp), ctypes.byref(ci), ctypes.byref(v))
     n = nnz.value
     return _take(rp, M + 1, np.int32), _take(ci, n, np.int32), _take(v, n, np.uint16).view(np.float16)
+
+
+def ref_mtx_to_csr(path: str, zero_based=True, pattern_only=False):
+    """The reference's mtx_input_to_CSR on a file: (M, K, row_ptr, col, vals fp16)."""
+    R = ref()
+    M, K, nnz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rp, ci = ctypes.POINTER(_I)(), ctypes.POINTER(_I)()
+    va = ctypes.POINTER(ctypes.c_uint16)()
+    rc = R.ref_mtx_to_csr(path.encode(), int(zero_based), int(pattern_only), ctypes.byref(M), ctypes.byref(K),
+                          ctypes.byref(nnz), ctypes.byref(rp), ctypes.byref(ci), ctypes.byref(va))
+    if rc != 0:
+        raise OSError(path)
+    n = nnz.value
+    return (M.value, K.value, _take(rp, M.value + 1, np.int32), _take(ci, n, np.int32),
+            _take(va, n, np.uint16).view(np.float16))
+
+
+def ref_mtx_to_dense(path: str, zero_based=True):
+    """The reference's mtx_input_to_Dense on a file: M x K fp16."""
+    R = ref()
+    M, K = ctypes.c_int(), ctypes.c_int()
+    mat = ctypes.POINTER(ctypes.c_uint16)()
+    rc = R.ref_mtx_to_dense(path.encode(), int(zero_based), ctypes.byref(M), ctypes.byref(K), ctypes.byref(mat))
+    if rc != 0:
+        raise OSError(path)
+    return _take(mat, M.value * K.value, np.uint16).view(np.float16).reshape(M.value, K.value)
 
 
 def ref_csr_to_dense(M, K, row_ptr, col_idx, vals):
@@ -348,6 +404,19 @@ def ref_cusparse_spmm(A, B, C=None, n_iter=1):
     out = np.zeros((M, N), np.float32) if C is None else _c(C, np.float32).copy()
     ms = ctypes.c_double(-1.0)
     ref().ref_cusparse_spmm(Ab.ctypes.data, Bb.ctypes.data, out.ctypes.data, M, N, K, n_iter, ctypes.byref(ms))
+    return out, ms.value
+
+
+def ref_cusparse_blockspmm(A, B, bs, C=None, n_iter=1):
+    """The reference's Blocked-ELL comparator (shapes must be multiples of bs:
+    the reference reads its host buffers with the padded strides otherwise)."""
+    Ab, Bb = f16_bits(A), f16_bits(B)
+    M, K = Ab.shape
+    N = Bb.shape[1]
+    out = np.zeros((M, N), np.float32) if C is None else _c(C, np.float32).copy()
+    ms = ctypes.c_double(-1.0)
+    ref().ref_cusparse_blockspmm(Ab.ctypes.data, Bb.ctypes.data, out.ctypes.data, M, N, K, n_iter, bs,
+                                 ctypes.byref(ms))
     return out, ms.value
 
 

@@ -614,3 +614,87 @@ void orc_quant_cols(int K, int N, const uint16_t *B, int ldb, uint8_t *q, int ld
     for (int k = 0; k < K; k++)
         for (int n = 0; n < N; n++) q[(size_t)k * ldq + n] = orc_f32_to_e4m3(orc_h2f(B[(size_t)k * ldb + n]) / scale[n]);
 }
+
+/* ---------------------------------------------------------------------------
+ * MatrixMarket coordinate text (restates src/file_input.cu:63-134,
+ * mtx_input_to_CSR, and :8-62, mtx_input_to_Dense, through `missing`): '%'
+ * lines are comments; the first other line is "rows cols nnz"; each further
+ * non-blank line is "r c [v]", 1-based unless zero_based. pattern_only: v =
+ * 1.0; else a missing v is `missing`. Rows in order, file order within a row.
+ * Returns nnz, or -1 when the text is malformed (no header, a bad entry line,
+ * an index out of range, a count different from the header). Output arrays
+ * are malloc'd (row_ptr M+1, col nnz, val nnz FP16 bits).
+ * ------------------------------------------------------------------------- */
+long orc_mtx_parse(const char *text, long len, int zero_based, int pattern_only, float missing, int *M, int *K,
+                   int **row_ptr_out, int **col_out, uint16_t **val_out)
+{
+    const char *p = text, *end = text + len;
+    long rows = -1, cols = -1, meta = -1, n = 0;
+    int *er = NULL, *ec = NULL;
+    float *ev = NULL;
+    while (p < end) {
+        const char *q = p;
+        while (q < end && *q != '\n') q++;
+        /* copy the line to a NUL-terminated buffer */
+        char buf[512];
+        long L = (long)(q - p);
+        if (L > 511) L = 511;
+        memcpy(buf, p, (size_t)L);
+        buf[L] = 0;
+        p = q < end ? q + 1 : q;
+        char *s = buf;
+        while (*s == ' ' || *s == '\t' || *s == '\r') s++;
+        if (*s == 0 || *s == '%') continue;
+        char *e1, *e2;
+        if (rows < 0) {
+            rows = strtol(s, &e1, 10);
+            if (e1 == s) goto bad;
+            cols = strtol(e1, &e2, 10);
+            if (e2 == e1) goto bad;
+            meta = strtol(e2, &s, 10);
+            if (s == e2 || rows < 0 || cols < 0 || meta < 0) goto bad;
+            er = (int *)malloc(sizeof(int) * (size_t)(meta + 1));
+            ec = (int *)malloc(sizeof(int) * (size_t)(meta + 1));
+            ev = (float *)malloc(sizeof(float) * (size_t)(meta + 1));
+            continue;
+        }
+        long r = strtol(s, &e1, 10);
+        if (e1 == s) goto bad;
+        long c = strtol(e1, &e2, 10);
+        if (e2 == e1) goto bad;
+        float v = pattern_only ? 1.0f : missing;
+        if (!pattern_only) {
+            char *t = e2, *e3;
+            while (*t == ' ' || *t == '\t') t++;
+            if (*t == '+' || *t == '-' || *t == '.' || (*t >= '0' && *t <= '9')) {
+                const float x = strtof(t, &e3);
+                if (e3 != t) v = x;
+            }
+        }
+        if (!zero_based) { r--; c--; }
+        if (r < 0 || r >= rows || c < 0 || c >= cols || n >= meta) goto bad;
+        er[n] = (int)r; ec[n] = (int)c; ev[n] = v; n++;
+    }
+    if (rows < 0 || n != meta) goto bad;
+    {
+        int *rp = (int *)calloc((size_t)rows + 1, sizeof(int));
+        int *co = (int *)malloc(sizeof(int) * (size_t)(n + 1));
+        uint16_t *va = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)(n + 1));
+        for (long i = 0; i < n; i++) rp[er[i] + 1]++;
+        for (long i = 0; i < rows; i++) rp[i + 1] += rp[i];
+        int *fill = (int *)malloc(sizeof(int) * (size_t)(rows + 1));
+        memcpy(fill, rp, sizeof(int) * (size_t)(rows + 1));
+        for (long i = 0; i < n; i++) {           /* stable: file order within a row */
+            const int j = fill[er[i]]++;
+            co[j] = ec[i];
+            va[j] = orc_f2h(ev[i]);
+        }
+        free(fill); free(er); free(ec); free(ev);
+        *M = (int)rows; *K = (int)cols;
+        *row_ptr_out = rp; *col_out = co; *val_out = va;
+        return n;
+    }
+bad:
+    free(er); free(ec); free(ev);
+    return -1;
+}

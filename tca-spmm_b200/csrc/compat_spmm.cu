@@ -7,6 +7,8 @@
 #include <cusparse.h>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
+#include <vector>
 #include "tca_internal.cuh"
 #include "tca_spmm_compat.h"
 
@@ -178,6 +180,120 @@ done:
     cudaFree(dA);
     cudaFree(dB);
     cudaFree(dC);
+    if (st != TCA_OK)
+        tca::compat_report(st);
+}
+
+// src/spmm_cusparse.cu:181-445: the cuSPARSE Blocked-ELL comparator. A (dense,
+// M x K) is cut into ell_block_size square blocks; every block row keeps the
+// blocks that hold a nonzero, padded to the widest block row with empty
+// slots (column index -1); cusparseSpMM on that Blocked-ELL matrix with FP16
+// A and B, FP32 C and compute, CUSPARSE_SPMM_ALG_DEFAULT, num_iter timed calls
+// after one untimed call. M and K are padded to multiples of the block size
+// with zeros (the reference pads the shapes too, but reads the unpadded host
+// A and B with the padded strides); C gets the first M rows back.
+void perform_cuSPARSE_BlockSpMM(half *A, half *B, float *C, int M, int N, int K, int num_iter, int ell_block_size,
+                                double *elapsed)
+{
+    int st = TCA_OK;
+    const int bs = ell_block_size;
+    int *d_cols = nullptr;
+    half *d_vals = nullptr, *d_B = nullptr;
+    float *d_C = nullptr;
+    void *d_buf = nullptr;
+    size_t buf_bytes = 0;
+    cusparseHandle_t h = nullptr;
+    cusparseSpMatDescr_t mA = nullptr;
+    cusparseDnMatDescr_t mB = nullptr, mC = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float alpha = 1.f, beta = 0.f, ms = 0.f;
+    std::vector<int> cols;
+    std::vector<half> vals, Bp;
+    int brows = 0, bcols = 0, width = 0, Mp = 0, Kp = 0;
+    if (bs <= 0 || M <= 0 || K <= 0 || N <= 0 || !A || !B || !C) {
+        st = set_error(TCA_ERR_INVALID_ARG, "perform_cuSPARSE_BlockSpMM: invalid sizes or buffers");
+        goto done;
+    }
+    if (num_iter < 1)
+        num_iter = 1;
+    brows = (M + bs - 1) / bs;
+    bcols = (K + bs - 1) / bs;
+    Mp = brows * bs;
+    Kp = bcols * bs;
+    {
+        // occupied blocks per block row, in column order
+        std::vector<std::vector<int>> occ((size_t)brows);
+        for (int bi = 0; bi < brows; bi++) {
+            for (int bj = 0; bj < bcols; bj++) {
+                bool any = false;
+                for (int i = bi * bs; i < std::min(M, (bi + 1) * bs) && !any; i++)
+                    for (int j = bj * bs; j < std::min(K, (bj + 1) * bs); j++)
+                        if (__half2float(A[(size_t)i * K + j]) != 0.f) { any = true; break; }
+                if (any) occ[bi].push_back(bj);
+            }
+            width = std::max(width, (int)occ[bi].size());
+        }
+        width = std::max(width, 1);
+        cols.assign((size_t)brows * width, -1);
+        vals.assign((size_t)Mp * width * bs, __float2half(0.f));
+        for (int bi = 0; bi < brows; bi++)
+            for (int s = 0; s < (int)occ[bi].size(); s++) {
+                const int bj = occ[bi][s];
+                cols[(size_t)bi * width + s] = bj;
+                for (int r = 0; r < bs; r++) {
+                    const int i = bi * bs + r;
+                    if (i >= M) break;
+                    for (int c = 0; c < bs; c++) {
+                        const int j = bj * bs + c;
+                        if (j < K) vals[(size_t)i * width * bs + (size_t)s * bs + c] = A[(size_t)i * K + j];
+                    }
+                }
+            }
+        Bp.assign((size_t)Kp * N, __float2half(0.f));
+        std::copy(B, B + (size_t)K * N, Bp.begin());
+    }
+    COMPAT_CUDA(cudaMalloc(&d_cols, sizeof(int) * cols.size()));
+    COMPAT_CUDA(cudaMalloc(&d_vals, sizeof(half) * vals.size()));
+    COMPAT_CUDA(cudaMalloc(&d_B, sizeof(half) * Bp.size()));
+    COMPAT_CUDA(cudaMalloc(&d_C, sizeof(float) * (size_t)Mp * N));
+    COMPAT_CUDA(cudaMemcpy(d_cols, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice));
+    COMPAT_CUDA(cudaMemcpy(d_vals, vals.data(), sizeof(half) * vals.size(), cudaMemcpyHostToDevice));
+    COMPAT_CUDA(cudaMemcpy(d_B, Bp.data(), sizeof(half) * Bp.size(), cudaMemcpyHostToDevice));
+    COMPAT_SPARSE(cusparseCreate(&h));
+    COMPAT_SPARSE(cusparseCreateBlockedEll(&mA, Mp, Kp, bs, (int64_t)width * bs, d_cols, d_vals, CUSPARSE_INDEX_32I,
+                                           CUSPARSE_INDEX_BASE_ZERO, CUDA_R_16F));
+    COMPAT_SPARSE(cusparseCreateDnMat(&mB, Kp, N, N, d_B, CUDA_R_16F, CUSPARSE_ORDER_ROW));
+    COMPAT_SPARSE(cusparseCreateDnMat(&mC, Mp, N, N, d_C, CUDA_R_32F, CUSPARSE_ORDER_ROW));
+    COMPAT_SPARSE(cusparseSpMM_bufferSize(h, CUSPARSE_OPERATION_NON_TRANSPOSE, CUSPARSE_OPERATION_NON_TRANSPOSE,
+                                          &alpha, mA, mB, &beta, mC, CUDA_R_32F, CUSPARSE_SPMM_ALG_DEFAULT,
+                                          &buf_bytes));
+    COMPAT_CUDA(cudaMalloc(&d_buf, buf_bytes > 0 ? buf_bytes : 1));
+    COMPAT_SPARSE(cusparseSpMM(h, CUSPARSE_OPERATION_NON_TRANSPOSE, CUSPARSE_OPERATION_NON_TRANSPOSE, &alpha, mA, mB,
+                               &beta, mC, CUDA_R_32F, CUSPARSE_SPMM_ALG_DEFAULT, d_buf));
+    COMPAT_CUDA(cudaEventCreate(&e0));
+    COMPAT_CUDA(cudaEventCreate(&e1));
+    COMPAT_CUDA(cudaEventRecord(e0));
+    for (int i = 0; i < num_iter; i++)
+        COMPAT_SPARSE(cusparseSpMM(h, CUSPARSE_OPERATION_NON_TRANSPOSE, CUSPARSE_OPERATION_NON_TRANSPOSE, &alpha,
+                                   mA, mB, &beta, mC, CUDA_R_32F, CUSPARSE_SPMM_ALG_DEFAULT, d_buf));
+    COMPAT_CUDA(cudaEventRecord(e1));
+    COMPAT_CUDA(cudaEventSynchronize(e1));
+    COMPAT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (elapsed)
+        *elapsed = (double)ms / num_iter;
+    COMPAT_CUDA(cudaMemcpy(C, d_C, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToHost));
+done:
+    if (mA) cusparseDestroySpMat(mA);
+    if (mB) cusparseDestroyDnMat(mB);
+    if (mC) cusparseDestroyDnMat(mC);
+    if (h) cusparseDestroy(h);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d_buf);
+    cudaFree(d_cols);
+    cudaFree(d_vals);
+    cudaFree(d_B);
+    cudaFree(d_C);
     if (st != TCA_OK)
         tca::compat_report(st);
 }

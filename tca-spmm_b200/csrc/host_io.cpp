@@ -169,6 +169,100 @@ void compat_fail(int st)
         std::exit(EXIT_FAILURE);
 }
 
+// MatrixMarket coordinate text as the reference's mtx_input_to_CSR /
+// mtx_input_to_Dense read it (src/file_input.cu:8-134): '%' lines are
+// comments, the first other line is "rows cols nnz", every further line is
+// "r c [v]" (1-based unless zero_based). pattern_only ignores a value and uses
+// 1.0; otherwise a missing value is `missing` (0.0 in the reference's CSR
+// reader, 1.0 in its dense reader). Entries keep the file's order within a
+// row (no sorting, duplicates kept). Where the reference has undefined
+// behaviour -- blank lines, '%' lines after the header, indices out of range,
+// a count different from the header -- this returns TCA_ERR_FORMAT (blank
+// lines are skipped).
+struct MtxEntry {
+    int r, c;
+    float v;
+};
+
+// Whitespace-separated tokens of one line, read as stream extraction would.
+struct WsTok {
+    const char *p, *end;
+    void skip() { while (p < end && (*p == ' ' || *p == '\t' || *p == '\r' || *p == '\v' || *p == '\f')) p++; }
+    bool next_int(long long *out)
+    {
+        skip();
+        if (p >= end) return false;
+        char *stop = nullptr;
+        errno = 0;
+        const long long v = std::strtoll(p, &stop, 10);
+        if (stop == p || errno == ERANGE) return false;
+        p = stop;
+        *out = v;
+        return true;
+    }
+    // false (value untouched) when no number starts here, as `>> float` leaves it
+    bool next_float(float *out)
+    {
+        skip();
+        if (p >= end) return false;
+        const char c0 = *p;
+        if (!(c0 == '+' || c0 == '-' || c0 == '.' || (c0 >= '0' && c0 <= '9'))) return false;
+        std::string tok(p, (size_t)(end - p));
+        char *stop = nullptr;
+        const float v = std::strtof(tok.c_str(), &stop);
+        if (stop == tok.c_str()) return false;
+        p += stop - tok.c_str();
+        *out = v;
+        return true;
+    }
+};
+
+int parse_mtx(const char *text, size_t len, bool zero_based, bool pattern_only, float missing, int *M, int *K,
+              int *nnz, std::vector<MtxEntry> &ent)
+{
+    const char *p = text, *end = text + len;
+    bool have_header = false;
+    long long rows = 0, cols = 0, meta = 0;
+    ent.clear();
+    int line_no = 0;
+    while (p < end) {
+        const char *q = p;
+        while (q < end && *q != '\n') q++;
+        WsTok t{p, q};
+        p = q < end ? q + 1 : q;
+        line_no++;
+        t.skip();
+        if (t.p >= t.end) continue;    // blank line
+        if (*t.p == '%') continue;     // comment (the reference skips them before the header only)
+        if (!have_header) {
+            if (!t.next_int(&rows) || !t.next_int(&cols) || !t.next_int(&meta) || rows < 0 || cols < 0 || meta < 0 ||
+                rows > INT32_MAX || cols > INT32_MAX || meta > INT32_MAX)
+                return set_error(TCA_ERR_FORMAT, "MatrixMarket line %d: expected \"rows cols nnz\"", line_no);
+            have_header = true;
+            ent.reserve((size_t)meta);
+            continue;
+        }
+        long long r, c;
+        if (!t.next_int(&r) || !t.next_int(&c))
+            return set_error(TCA_ERR_FORMAT, "MatrixMarket line %d: expected \"row col [value]\"", line_no);
+        float v = pattern_only ? 1.0f : missing;
+        if (!pattern_only) t.next_float(&v);
+        if (!zero_based) { r--; c--; }
+        if (r < 0 || r >= rows || c < 0 || c >= cols)
+            return set_error(TCA_ERR_FORMAT, "MatrixMarket line %d: entry (%lld, %lld) outside %lld x %lld", line_no,
+                             r, c, rows, cols);
+        ent.push_back(MtxEntry{(int)r, (int)c, v});
+    }
+    if (!have_header) return set_error(TCA_ERR_FORMAT, "MatrixMarket text has no \"rows cols nnz\" line");
+    if ((long long)ent.size() != meta)
+        return set_error(TCA_ERR_FORMAT, "MatrixMarket header announces %lld entries, the text has %zu", meta,
+                         ent.size());
+    *M = (int)rows;
+    *K = (int)cols;
+    *nnz = (int)meta;
+    return TCA_OK;
+}
+
 } // namespace
 
 bool compat_exit_on_error() { return g_exit_on_error; }
@@ -205,6 +299,41 @@ int tca_smtx_read(const char *path, int *M, int *K, int *nnz, int **row_ptr, int
     std::string s;
     TCA_TRY(read_file(path, s));
     return tca_smtx_parse(s.data(), s.size(), M, K, nnz, row_ptr, col_idx, vals_f16);
+}
+
+int tca_mtx_parse(const char *text, size_t len, int zero_based, int pattern_only, float missing_value, int *M,
+                  int *K, int *nnz, int **row_ptr, int **col_idx, void **vals_f16)
+{
+    clear_error();
+    if (!text || !M || !K || !nnz) return set_error(TCA_ERR_INVALID_ARG, "NULL argument");
+    std::vector<MtxEntry> ent;
+    TCA_TRY(parse_mtx(text, len, zero_based != 0, pattern_only != 0, missing_value, M, K, nnz, ent));
+    // rows in order, each row's entries in file order (a stable counting sort)
+    std::vector<int> rp((size_t)*M + 1, 0), ci(ent.size());
+    std::vector<uint16_t> v(ent.size());
+    for (const MtxEntry &e : ent) rp[(size_t)e.r + 1]++;
+    for (int i = 0; i < *M; i++) rp[(size_t)i + 1] += rp[i];
+    std::vector<int> fill(rp.begin(), rp.end() - 1);
+    for (const MtxEntry &e : ent) {
+        const int j = fill[e.r]++;
+        ci[j] = e.c;
+        v[j] = __half_as_ushort(__float2half_rn(e.v));
+    }
+    if (row_ptr) *row_ptr = dup_malloc(rp);
+    if (col_idx) *col_idx = dup_malloc(ci);
+    if (vals_f16) *vals_f16 = dup_malloc(v);
+    return TCA_OK;
+}
+
+int tca_mtx_read(const char *path, int zero_based, int pattern_only, float missing_value, int *M, int *K, int *nnz,
+                 int **row_ptr, int **col_idx, void **vals_f16)
+{
+    clear_error();
+    if (!path) return set_error(TCA_ERR_INVALID_ARG, "path is NULL");
+    std::string s;
+    TCA_TRY(read_file(path, s));
+    return tca_mtx_parse(s.data(), s.size(), zero_based, pattern_only, missing_value, M, K, nnz, row_ptr, col_idx,
+                         vals_f16);
 }
 
 int tca_smtx_write(const char *path, int M, int K, int nnz, const int *row_ptr, const int *col_idx,
@@ -472,4 +601,53 @@ int format_conversion(mat_format in, mat_format out, const COO *src, half **dst)
     const int st = format_conversion(csr, dense, c, dst);
     destroy_csr(c);
     return st;
+}
+
+// ------------------------------------------------------------------ MatrixMarket drop-ins
+
+Arguments::Arguments()
+    : M(1024), N(1024), K(1024), num_iter(10), pattern_only(false), input_is_zero_based(true),
+      input_file_exists(false), target_sparsity(0.8f), tolerance(1e-3f), a_type(fp16), b_type(fp16), c_type(fp32),
+      input_fname(nullptr), ell_block_size(32)
+{
+}
+
+static std::string slurp(std::ifstream &fin)
+{
+    std::ostringstream ss;
+    ss << fin.rdbuf();
+    return ss.str();
+}
+
+void mtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg)
+{
+    const std::string s = slurp(fin);
+    const Arguments def;
+    const Arguments &a = arg ? *arg : def;
+    int M, K, nnz, *rp = nullptr, *ci = nullptr;
+    void *v = nullptr;
+    const int st = tca_mtx_parse(s.data(), s.size(), a.input_is_zero_based, a.pattern_only, 0.0f, &M, &K, &nnz, &rp,
+                                 &ci, &v);
+    if (st != TCA_OK) { compat_report(st); *csr_mat = nullptr; return; }
+    *csr_mat = make_csr(M, K, nnz, rp, ci, (half *)v);
+}
+
+void mtx_input_to_Dense(std::ifstream &fin, half **mat, Arguments *arg)
+{
+    const std::string s = slurp(fin);
+    const Arguments def;
+    const Arguments &a = arg ? *arg : def;
+    int M, K, nnz, *rp = nullptr, *ci = nullptr;
+    void *v = nullptr;
+    // the reference's dense reader always reads a value and keeps 1.0 where there is none
+    const int st = tca_mtx_parse(s.data(), s.size(), a.input_is_zero_based, 0, 1.0f, &M, &K, &nnz, &rp, &ci, &v);
+    if (st != TCA_OK) { compat_report(st); *mat = nullptr; return; }
+    *mat = (half *)std::malloc(sizeof(half) * (size_t)M * K + 1);
+    tca_csr_to_dense(M, K, nnz, rp, ci, v, *mat);
+    std::free(rp); std::free(ci); std::free(v);
+}
+
+void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg)
+{
+    smtx_input_to_CSR(fin, csr_mat, static_cast<void *>(arg));
 }

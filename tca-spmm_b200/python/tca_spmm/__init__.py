@@ -79,6 +79,8 @@ _SIGS = {
     "tca_last_error_string": ([], ctypes.c_char_p),
     "tca_status_string": ([_I], ctypes.c_char_p),
     "tca_spmm_csr": ([_P, _P, _P, _I, _I, _I, _P, _I, _I, _P, _I, _I, _F, _F, _U, _VP], _I),
+    "tca_spmm_csr_f64": ([_P, _P, _P, _I, _I, _I, _P, _I, _I, _P, _I, ctypes.c_double, ctypes.c_double, _U,
+                          _VP], _I),
     "tca_plan_opts_default": ([ctypes.POINTER(PlanOpts)], None),
     "tca_plan_create": ([_P, _P, _P, _I, _I, _I, ctypes.POINTER(PlanOpts), _VP, ctypes.POINTER(_VP)], _I),
     "tca_plan_update_values": ([_VP, _P, _VP], _I),
@@ -104,6 +106,11 @@ _SIGS = {
     "tca_batch_graph_launch": ([_VP, _VP], _I),
     "tca_batch_graph_destroy": ([_VP], _I),
     "tca_batch_autotune": ([ctypes.POINTER(BatchItem), _I, _I, _I, _I, _VP], _I),
+    "tca_mtx_parse": ([ctypes.c_char_p, ctypes.c_size_t, _I, _I, _F, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                       ctypes.POINTER(_I), ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP)], _I),
+    "tca_mtx_read": ([ctypes.c_char_p, _I, _I, _F, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                      ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP)], _I),
+    "tca_free": ([_VP], None),
     "tca_spmm_host": ([_P, _P, _P, _I, _I, _I, _P, _I, _P, _I, _U, _I, ctypes.POINTER(ctypes.c_double)], _I),
 }
 
@@ -450,6 +457,46 @@ def quantize_b_fp8(B, stream=None):
     scale = torch.empty(N, dtype=torch.float32, device=B.device)
     _check(lib().tca_quantize_b_fp8(_ptr(B), B.stride(0), K, N, _ptr(Bq), ldq, _ptr(scale), _stream_handle(stream)))
     return Bq, scale
+
+
+def mtx_read(path, zero_based=False, pattern_only=False, missing_value=0.0):
+    """A MatrixMarket coordinate file as host CSR (tca_mtx_read): (M, K,
+    row_ptr int32, col_idx int32, vals float16), rows in order, file order
+    within a row, as the reference's mtx_input_to_CSR reads it."""
+    L = lib()
+    M, K, nnz = _I(), _I(), _I()
+    rp, ci, v = _VP(), _VP(), _VP()
+    _check(L.tca_mtx_read(str(path).encode(), int(zero_based), int(pattern_only), missing_value, ctypes.byref(M),
+                          ctypes.byref(K), ctypes.byref(nnz), ctypes.byref(rp), ctypes.byref(ci), ctypes.byref(v)))
+
+    def take(ptr, n, dt):
+        a = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(np.ctypeslib.as_ctypes_type(dt))),
+                                  shape=(max(n, 1),))[:n].copy()
+        L.tca_free(ptr)
+        return a
+
+    n = nnz.value
+    return (M.value, K.value, take(rp, M.value + 1, np.int32), take(ci, n, np.int32),
+            take(v, n, np.uint16).view(np.float16))
+
+
+def spmm_csr_f64(row_ptr, col_idx, vals, B, K=None, out=None, alpha=1.0, beta=0.0, keep_empty_rows=False,
+                 stream=None):
+    """FP64 forward from CSR on CUDA cores (tca_spmm_csr_f64): float64 values,
+    B and output."""
+    torch = _torch()
+    if B.dim() != 2 or B.dtype != torch.float64 or not B.is_cuda or B.stride(1) != 1:
+        raise ValueError("B must be a 2-D CUDA float64 tensor with unit column stride")
+    M = row_ptr.numel() - 1
+    N = B.shape[1]
+    if out is None:
+        out = torch.empty((M, N), dtype=torch.float64, device=B.device)
+    K = B.shape[0] if K is None else K
+    flags = FLAG_KEEP_EMPTY_ROWS if keep_empty_rows else 0
+    _check(lib().tca_spmm_csr_f64(_ptr(row_ptr), _ptr(col_idx), _ptr(vals), M, K, col_idx.numel(), _ptr(B),
+                                  B.stride(0), N, _ptr(out), out.stride(0), alpha, beta, flags,
+                                  _stream_handle(stream)))
+    return out
 
 
 def spmm_host(row_ptr: np.ndarray, col_idx: np.ndarray, vals: np.ndarray, K: int, B: np.ndarray,

@@ -13,6 +13,9 @@ oracle/_ref/libtcaref.so (`make -C oracle ref`):
     c2d_<i>_dense        convert_csr_to_dense (src/miscalleneous.cu:66-81)
     gemm_<i>_*           naive_gemm (src/miscalleneous.cu:114-134) on a seeded
                          sparse A (dense storage) and B
+  mtx_*.mtx              seeded MatrixMarket files (written by this script)
+    mtx_<i>_csr_*        mtx_input_to_CSR (src/file_input.cu:63-134) on mtx_<i>.mtx
+    mtx_<i>_dense        mtx_input_to_Dense (src/file_input.cu:8-62) on mtx_<i>.mtx
 
 Run from the repository root:  python tests/golden/make_golden.py
 """
@@ -73,6 +76,35 @@ def dense_case(rng, M, K, density):
     return A
 
 
+def write_mtx(path, rng, M, K, n, one_based, with_values, missing_every=0):
+    """Coordinate MatrixMarket text: a banner and a comment, "M K n", then n
+    entries in random order (rows and columns unsorted, some duplicates), a
+    value on each line unless with_values is False or the line is one of every
+    missing_every lines."""
+    rows = rng.integers(0, M, n)
+    cols = rng.integers(0, K, n)
+    if n > 4:
+        rows[1], cols[1] = rows[0], cols[0]  # a duplicate entry
+    vals = rng.standard_normal(n) * rng.choice([1e-3, 1.0, 300.0], n)
+    b = 1 if one_based else 0
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate " + ("real" if with_values else "pattern") + " general\n")
+        f.write("% generated by make_golden.py\n")
+        f.write(f"{M} {K} {n}\n")
+        for i in range(n):
+            line = f"{rows[i] + b} {cols[i] + b}"
+            if with_values and not (missing_every and i % missing_every == 0):
+                line += f" {vals[i]:.7g}"
+            f.write(line + "\n")
+
+
+MTX_CASES = [  # (M, K, n, one_based, with_values, missing_every, pattern_only)
+    (40, 30, 120, True, True, 7, False),
+    (25, 50, 60, True, False, 0, True),
+    (64, 16, 90, False, True, 0, False),
+]
+
+
 def main():
     subprocess.run(["make", "-C", str(ROOT / "oracle"), "all", "ref"], check=True)
     rng = np.random.default_rng(20240601)
@@ -97,6 +129,16 @@ def main():
         B = rng.uniform(-1, 1, size=(K, N)).astype(np.float16)
         g[f"gemm_{i}_A"], g[f"gemm_{i}_B"] = A, B
         g[f"gemm_{i}_C"] = oracle.ref_naive_gemm(A, B)
+    mrng = np.random.default_rng(20250301)
+    for i, (M, K, n, one_based, with_values, missing_every, pattern_only) in enumerate(MTX_CASES):
+        path = OUT / f"mtx_{i}.mtx"
+        write_mtx(path, mrng, M, K, n, one_based, with_values, missing_every)
+        with oracle.quiet_stdout():
+            m, k, rp, ci, v = oracle.ref_mtx_to_csr(str(path), zero_based=not one_based, pattern_only=pattern_only)
+            D = oracle.ref_mtx_to_dense(str(path), zero_based=not one_based)
+        g[f"mtx_{i}_csr_shape"] = np.array([m, k], np.int64)
+        g[f"mtx_{i}_csr_row_ptr"], g[f"mtx_{i}_csr_col"], g[f"mtx_{i}_csr_val"] = rp, ci, v
+        g[f"mtx_{i}_dense"] = D
     np.savez_compressed(OUT / "golden.npz", **g)
     print("wrote", OUT / "golden.npz", len(g), "arrays")
 

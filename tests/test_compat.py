@@ -137,3 +137,74 @@ def test_reference_style_driver_runs(tmp_path, cuda, case, N):
                        timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "our: [" in r.stdout
+
+
+BLOCK_DRIVER = r"""
+#include <cstdio>
+#include <vector>
+#include "tca_spmm_compat.h"
+// reads M N K bs, then A (M*K) and B (K*N) FP16 bits from argv[1]; writes C (FP32) to argv[2]
+int main(int argc, char **argv)
+{
+    FILE *f = fopen(argv[1], "rb");
+    int d[4];
+    if (fread(d, sizeof(int), 4, f) != 4) return 2;
+    const int M = d[0], N = d[1], K = d[2], bs = d[3];
+    std::vector<half> A((size_t)M * K), B((size_t)K * N);
+    if (fread(A.data(), 2, A.size(), f) != A.size() || fread(B.data(), 2, B.size(), f) != B.size()) return 3;
+    fclose(f);
+    std::vector<float> C((size_t)M * N, 0.f);
+    double ms = -1;
+    perform_cuSPARSE_BlockSpMM(A.data(), B.data(), C.data(), M, N, K, 3, bs, &ms);
+    FILE *g = fopen(argv[2], "wb");
+    fwrite(C.data(), sizeof(float), C.size(), g);
+    fclose(g);
+    printf("%f\n", ms);
+    return ms > 0 ? 0 : 4;
+}
+"""
+
+
+def _block_case(rng, M, K, N, bs, keep):
+    A = np.zeros((M, K), np.float16)
+    for bi in range(-(-M // bs)):
+        for bj in range(-(-K // bs)):
+            if rng.random() < keep:
+                blk = (rng.standard_normal((bs, bs)) * 0.3).astype(np.float16)
+                blk[rng.random((bs, bs)) < 0.5] = 0
+                A[bi * bs:(bi + 1) * bs, bj * bs:(bj + 1) * bs] = blk[:min(bs, M - bi * bs), :min(bs, K - bj * bs)]
+    B = rng.uniform(-1, 1, (K, N)).astype(np.float16)
+    return A, B
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("M,K,N,bs", [(256, 128, 64, 32), (200, 130, 48, 16), (512, 512, 128, 64)])
+def test_blocked_ell_comparator(tmp_path, cuda, M, K, N, bs):
+    """perform_cuSPARSE_BlockSpMM (the reference's Blocked-ELL comparator
+    signature) against the FP64 product and, where the shapes are multiples of
+    the block size, the reference's own comparator (relative Frobenius <= 1e-3)."""
+    src = tmp_path / "block.cu"
+    src.write_text(BLOCK_DRIVER)
+    exe = tmp_path / "block"
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    r = subprocess.run([nvcc, "-std=c++17", "-I", str(ROOT / "include"), str(src), "-L", str(PKG / "lib"),
+                        "-ltca_spmm", "-Xlinker", f"-rpath,{PKG / 'lib'}", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    A, B = _block_case(np.random.default_rng(M + K), M, K, N, bs, 0.3)
+    inp = tmp_path / "in.bin"
+    with open(inp, "wb") as f:
+        f.write(np.array([M, N, K, bs], np.int32).tobytes())
+        f.write(A.view(np.uint16).tobytes())
+        f.write(B.view(np.uint16).tobytes())
+    out = tmp_path / "out.bin"
+    subprocess.run([str(exe), str(inp), str(out)], check=True, capture_output=True, timeout=120)
+    C = np.fromfile(out, np.float32).reshape(M, N)
+    ref = A.astype(np.float64) @ B.astype(np.float64)
+    assert np.linalg.norm(C - ref) <= 1e-3 * np.linalg.norm(ref)
+    if M % bs == 0 and K % bs == 0:
+        from oracle import oracle
+        if oracle.ref_available():
+            with oracle.quiet_stdout():
+                Cr, _ = oracle.ref_cusparse_blockspmm(A, B, bs)
+            assert np.linalg.norm(C - Cr) <= 1e-3 * np.linalg.norm(Cr)
