@@ -147,11 +147,13 @@ int tca_batch_autotune(tca_batch_item_t *items, int n_items, int c_dtype, int pr
         std::vector<int> tiles = precision == TCA_PRECISION_E4M3 ? std::vector<int>{128, 256}
                                                                 : std::vector<int>{64, 128, 256};
         std::vector<int> cols = {2, 4, 8};
+        if (precision == TCA_PRECISION_F16)
+            cols.push_back(16); // the tensor-core item kernel
         for (int nt : tiles) {
             if (nt > 64 && nt / 2 >= N && !(precision == TCA_PRECISION_E4M3 && nt == 128))
                 continue; // a slice at least twice as wide as N only adds zero columns
             for (int w : cols) {
-                if (w > 2 && w * 16 > N)
+                if (w > 2 && w < 16 && w * 16 > N)
                     continue; // fewer than half of the lanes would have columns
                 tca_batch_item_t cand = items[i];
                 cand.n_tile = nt;

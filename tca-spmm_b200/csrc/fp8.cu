@@ -116,56 +116,127 @@ __device__ __forceinline__ void load8h(const QJob &q, int k, int n, bool vec, fl
     }
 }
 
-// Column absolute maxima (FP32 bit patterns order like the non-negative
-// values): thread = 8 consecutive columns, blockIdx.y = 32 rows of B.
-__global__ void k_col_absmax(const __grid_constant__ QBatch b)
+// The two B passes tile B into blocks of 64 rows x 256 columns: thread
+// (x, y) of a 32 x 8 block takes the 8 consecutive columns (one 16-byte
+// vector) 8 x of the block's columns in the 8 consecutive rows 8 y .. of its
+// rows, so that a warp reads whole 512-byte row segments; all 8 loads of a
+// thread are issued before the first is used (blockIdx.z = matrix).
+constexpr int kQTileRows = 64, kQTileCols = 256, kQRows = kQTileRows / 8;
+
+struct QTile {
+    int n, k0, k1;
+    bool fast; // full 16-byte vectors and all kQRows rows in range
+};
+
+__device__ __forceinline__ QTile q_tile(const QJob &q)
 {
-    const QJob &q = b.job[blockIdx.z];
-    const int n = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
-    const int k0 = blockIdx.y * 32;
-    if (n >= q.N || k0 >= q.K)
-        return;
-    const bool vec = vec8_ok(q);
-    const int k1 = min(q.K, k0 + 32);
-    float m[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    for (int k = k0; k < k1; k++) {
-        float v[8];
-        load8h(q, k, n, vec, v);
-#pragma unroll
-        for (int i = 0; i < 8; i++) m[i] = fmaxf(m[i], fabsf(v[i]));
-    }
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-        if (n + i < q.N)
-            atomicMax(q.colmax + n + i, __float_as_uint(m[i]));
+    QTile t;
+    t.n = blockIdx.x * kQTileCols + threadIdx.x * 8;
+    t.k0 = blockIdx.y * kQTileRows + threadIdx.y * kQRows;
+    t.k1 = min(q.K, t.k0 + kQRows);
+    t.fast = vec8_ok(q) && t.n + 8 <= q.N && t.k0 + kQRows <= q.K;
+    return t;
 }
 
-// Bq[k, n] = E4M3(B[k, n] / s[n]); thread = 8 consecutive columns, rows
-// blockIdx.y, + gridDim.y, ...
-__global__ void k_quant_cols(const __grid_constant__ QBatch b)
+__device__ __forceinline__ void load_rows8(const QJob &q, const QTile &t, uint4 *r)
+{
+#pragma unroll
+    for (int j = 0; j < kQRows; j++)
+        r[j] = __ldg(reinterpret_cast<const uint4 *>(q.B + (size_t)(t.k0 + j) * q.ldb + t.n));
+    asm volatile("" ::: "memory"); // every load issued before the first use
+}
+
+// Column absolute maxima (FP32 bit patterns order like the non-negative
+// values): per thread the maxima of its rows, per block the maxima over its
+// 8 row slices (shared memory), then one atomicMax per column and block.
+__global__ void __launch_bounds__(256) k_col_absmax(const __grid_constant__ QBatch b)
 {
     const QJob &q = b.job[blockIdx.z];
-    const int n = (blockIdx.x * blockDim.x + threadIdx.x) * 8;
-    if (n >= q.N)
+    if ((int)blockIdx.x * kQTileCols >= q.N || (int)blockIdx.y * kQTileRows >= q.K)
+        return; // whole block
+    __shared__ float s_m[8][8][32]; // [row slice][column in vector][vector]
+    const QTile t = q_tile(q);
+    float m[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (t.fast) {
+        uint4 r[kQRows];
+        load_rows8(q, t, r);
+#pragma unroll
+        for (int j = 0; j < kQRows; j++) {
+            const __half2 *h = reinterpret_cast<const __half2 *>(&r[j]);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const float2 f = __half22float2(h[i]);
+                m[2 * i] = fmaxf(m[2 * i], fabsf(f.x));
+                m[2 * i + 1] = fmaxf(m[2 * i + 1], fabsf(f.y));
+            }
+        }
+    } else if (t.n < q.N) {
+        const bool vec = vec8_ok(q);
+        for (int k = t.k0; k < t.k1; k++) {
+            float v[8];
+            load8h(q, k, t.n, vec, v);
+#pragma unroll
+            for (int i = 0; i < 8; i++) m[i] = fmaxf(m[i], fabsf(v[i]));
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) s_m[threadIdx.y][i][threadIdx.x] = m[i];
+    __syncthreads();
+    const int c = threadIdx.y * 32 + threadIdx.x; // column of the block: vector c / 8, element c % 8
+    float v = 0.f;
+#pragma unroll
+    for (int y = 0; y < 8; y++) v = fmaxf(v, s_m[y][c & 7][c >> 3]);
+    const int col = blockIdx.x * kQTileCols + c;
+    if (col < q.N && v > 0.f) // the maxima start at 0
+        atomicMax(q.colmax + col, __float_as_uint(v));
+}
+
+// Bq[k, n] = E4M3(B[k, n] / s[n]) over the thread's rows and columns.
+__global__ void __launch_bounds__(256) k_quant_cols(const __grid_constant__ QBatch b)
+{
+    const QJob &q = b.job[blockIdx.z];
+    const QTile t = q_tile(q);
+    if (t.n >= q.N || t.k0 >= q.K)
         return;
-    const bool vec = vec8_ok(q);
     float s[8];
 #pragma unroll
-    for (int i = 0; i < 8; i++) s[i] = n + i < q.N ? scale_of(__uint_as_float(q.colmax[n + i])) : 1.f;
-    for (int k = blockIdx.y; k < q.K; k += gridDim.y) {
+    for (int i = 0; i < 8; i++) s[i] = t.n + i < q.N ? scale_of(__uint_as_float(q.colmax[t.n + i])) : 1.f;
+    const bool st8 = (q.ldq & 7) == 0 && (reinterpret_cast<uintptr_t>(q.Bq) & 7u) == 0;
+    if (t.fast && st8) {
+        uint4 r[kQRows];
+        load_rows8(q, t, r);
+#pragma unroll
+        for (int j = 0; j < kQRows; j++) {
+            const __half2 *h = reinterpret_cast<const __half2 *>(&r[j]);
+            uint32_t w[2];
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                const float2 f0 = __half22float2(h[2 * p]), f1 = __half22float2(h[2 * p + 1]);
+                const uint32_t q0 = __nv_cvt_float2_to_fp8x2(make_float2(f0.x / s[4 * p], f0.y / s[4 * p + 1]),
+                                                             __NV_SATFINITE, __NV_E4M3);
+                const uint32_t q1 = __nv_cvt_float2_to_fp8x2(make_float2(f1.x / s[4 * p + 2], f1.y / s[4 * p + 3]),
+                                                             __NV_SATFINITE, __NV_E4M3);
+                w[p] = (q0 & 0xffffu) | (q1 << 16);
+            }
+            *reinterpret_cast<uint2 *>(q.Bq + (size_t)(t.k0 + j) * q.ldq + t.n) = make_uint2(w[0], w[1]);
+        }
+        return;
+    }
+    const bool vec = vec8_ok(q);
+    for (int k = t.k0; k < t.k1; k++) {
         float v[8];
-        load8h(q, k, n, vec, v);
+        load8h(q, k, t.n, vec, v);
         uint32_t lo = 0, hi = 0;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             lo |= (uint32_t)to_e4m3(v[i] / s[i]) << (8 * i);
             hi |= (uint32_t)to_e4m3(v[4 + i] / s[4 + i]) << (8 * i);
         }
-        uint8_t *dst = q.Bq + (size_t)k * q.ldq + n;
-        if (n + 8 <= q.N && (reinterpret_cast<uintptr_t>(dst) & 7u) == 0) {
+        uint8_t *dst = q.Bq + (size_t)k * q.ldq + t.n;
+        if (t.n + 8 <= q.N && (reinterpret_cast<uintptr_t>(dst) & 7u) == 0) {
             *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
         } else {
-            for (int i = 0; n + i < q.N && i < 8; i++) dst[i] = (uint8_t)((i < 4 ? lo : hi) >> (8 * (i & 3)));
+            for (int i = 0; t.n + i < q.N && i < 8; i++) dst[i] = (uint8_t)((i < 4 ? lo : hi) >> (8 * (i & 3)));
         }
     }
 }
@@ -190,9 +261,12 @@ int quantize_b_batch(const QBatch &b, cudaStream_t s)
     if (b.n == 0 || maxK == 0 || maxN == 0)
         return TCA_OK;
     const unsigned z = (unsigned)b.n;
+    const dim3 tiles(blocks(maxN, kQTileCols), blocks(maxK, kQTileRows), z), tile_threads(32, 8);
+    if (tiles.y > 65535u)
+        return set_error(TCA_ERR_INVALID_ARG, "B has too many rows to quantize (K=%d)", maxK);
     k_col_zero<<<dim3(blocks(maxN, 256), 1, z), 256, 0, s>>>(b);
-    k_col_absmax<<<dim3(blocks(blocks(maxN, 8), 128), blocks(maxK, 32), z), 128, 0, s>>>(b);
-    k_quant_cols<<<dim3(blocks(blocks(maxN, 8), 128), (unsigned)std::min(blocks(maxK, 8), 65535u), z), 128, 0, s>>>(b);
+    k_col_absmax<<<tiles, tile_threads, 0, s>>>(b);
+    k_quant_cols<<<tiles, tile_threads, 0, s>>>(b);
     k_col_scale<<<dim3(blocks(maxN, 256), 1, z), 256, 0, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;

@@ -655,9 +655,18 @@ namespace tca {
 int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
                          cudaStream_t s, void *const *events)
 {
+    // Without events the CUDA-core launches follow the tensor-core launch as
+    // programmatic dependents and run beside it; with events (which time each
+    // path alone) the two run one after the other.
     LaunchList tc, cc;
     TCA_TRY(launch_tc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &tc));
-    TCA_TRY(launch_cc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &cc));
+    int beside = 0;
+    for (int i = 0; !events && !tc.empty() && i < n_jobs; i++) {
+        int r = 0;
+        TCA_TRY(tc_block_regs(jobs[i].f8, &r));
+        beside = std::max(beside, r);
+    }
+    TCA_TRY(launch_cc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &cc, beside));
     // Under stream capture a plain record only orders the graph; an external
     // record becomes a graph node that records the event at every replay.
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;

@@ -140,14 +140,25 @@ using LaunchList = std::vector<std::function<int(cudaStream_t)>>;
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
                    cudaStream_t s, LaunchList *defer = nullptr);
 
+// Registers that one block of the tensor-core kernel holds on an SM (the
+// largest over its FP16 or its E4M3 instantiations).
+int tc_block_regs(bool f8, int *regs);
+
 // CUDA-core forward over the remaining windows of every job (all windows of
-// jobs without tc), in as few launches as the row widths allow.
+// jobs without tc), in as few launches as the row widths allow. beside_regs >
+// 0: the launches directly follow a tensor-core launch whose one block per SM
+// holds that many registers (tc_block_regs); they are issued as programmatic
+// dependents of it, which run beside it once its blocks are resident, with
+// grids sized to fit beside it. 0: ordinary launches.
 int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s, LaunchList *defer = nullptr);
+                   cudaStream_t s, LaunchList *defer = nullptr, int beside_regs = 0);
 
 // Prepares both launch lists, then issues them with optional events (4
 // caller-created cudaEvent_t or NULL) around the tensor-core and the
-// CUDA-core launches, so that the events bracket device work only.
+// CUDA-core launches, so that the events bracket device work only. Without
+// events, the CUDA-core launches run concurrently with the tensor-core launch
+// (programmatic dependents on the same stream; the two paths write disjoint
+// rows of C).
 int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
                          cudaStream_t s, void *const *events);
 

@@ -445,11 +445,19 @@ template <> struct BVec<2, true> { using T = unsigned short; };
 // products are formed exactly by the same mixed-precision FMA); the flush
 // multiplies the FP32 sum by row scale x column scale, as the tensor-core
 // epilogue does.
+//
+// Three blocks per SM (80 registers a thread): two of them fit beside the
+// tensor-core kernel's block when both paths run concurrently. U B loads are
+// in flight per lane: 8, or 4 at W = 8, which keeps the register budget
+// without spills.
 template <typename OutT, int W, bool F8>
-__global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(const __grid_constant__ CcBatch b)
+__global__ void __launch_bounds__(256, 3) spmm_cc_stream_kernel(const __grid_constant__ CcBatch b)
 {
     using V = typename BVec<W, F8>::T;
-    constexpr int U = 8;
+    constexpr int U = W == 8 ? 4 : 8;
+    // Launched as a programmatic dependent (beside the tensor-core kernel, or
+    // behind another CUDA-core launch): let the next launch start as well.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int n_warps = (int)gridDim.x * 8;
@@ -613,6 +621,12 @@ __global__ void __launch_bounds__(256, W == 8 ? 2 : 3) spmm_cc_stream_kernel(con
         d2 = d3;
         item += n_warps;
     }
+    // Complete no earlier than the launch this one depends on (a no-op for an
+    // ordinary launch): work after this kernel on the stream then also finds
+    // the tensor-core kernel done, whatever the stream's ordering rules for
+    // programmatic dependents. That kernel never waits on this one and all of
+    // its blocks were resident before this grid started, so the wait ends.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 template <typename OutT, int LPR>
@@ -685,10 +699,273 @@ int launch_cc_group(const CcBatch &b, cudaStream_t s)
     return TCA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core item kernel (mma.sync, FP16): the CUDA-core windows' work items
+// as tiny dense products. An item of R <= 31 rows and Z <= 32 nonzeros is
+// C_item[R x N] = A_item[R x Z] * B_item[Z x N], where A_item holds each
+// nonzero in its own column (row of the nonzero, position in the item) and
+// B_item is the item's gathered B rows. Per 64-column slice of N, the warp
+// stages B_item in shared memory (32 rows x 128 bytes, 16-byte chunks XOR-
+// swizzled by row), reads it with ldmatrix.trans as m16n8k16 B fragments and
+// issues 8 mma.sync per 16 rows and 16 nonzeros; A fragments come from the
+// nonzeros in lane registers by shuffle. The accumulators go through shared
+// memory so that every output row is stored as 128 contiguous bytes. A row
+// longer than 32 nonzeros (an item of its own) is walked 32 nonzeros at a
+// time into the same accumulators. Per output element this issues about a
+// third of the instructions of the shuffle-and-FMA stream kernel; the
+// products are exact in FP32 and sums accumulate in FP32.
+// ---------------------------------------------------------------------------
+constexpr int kMmaWarps = 8;
+constexpr int kCcMma = 16; // cc_cols value that selects this kernel
+constexpr int kMmaSliceCols = 64;
+constexpr int kMmaAccStride = 72; // floats per staged accumulator row (2-way bank conflicts at most)
+constexpr int kMmaWarpSmem = 16 * kMmaAccStride * 4; // >= 32 x 128 bytes of B staging
+
+__device__ __forceinline__ void mma_16816(float *d, const uint32_t *a, uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ void ldmatrix_x4_trans(uint32_t addr, uint32_t *r)
+{
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+
+template <typename OutT>
+__global__ void __launch_bounds__(kMmaWarps * 32, 2) spmm_cc_mma_kernel(const __grid_constant__ CcBatch b)
+{
+    __shared__ __align__(16) uint8_t s_all[kMmaWarps * kMmaWarpSmem];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint8_t *ws = s_all + wid * kMmaWarpSmem;
+    const uint32_t ws_addr = (uint32_t)__cvta_generic_to_shared(ws);
+    float *acc_s = reinterpret_cast<float *>(ws);
+    const int n_warps = (int)gridDim.x * kMmaWarps;
+    int item = (int)blockIdx.x * kMmaWarps + wid;
+    const int g = lane >> 2, c4 = lane & 3;
+
+    auto load_rows = [&](const ItemDesc &d, int &rs, int &orow) {
+        rs = 0;
+        orow = 0;
+        if (lane <= d.nrows && d.nrows > 0) {
+            const CcJob &a = b.job[d.job];
+            rs = __ldg(a.p_row_ptr + d.r0 + lane);
+            if (lane < d.nrows)
+                orow = __ldg(a.perm + d.r0 + lane);
+        }
+    };
+    auto load_nz = [&](const ItemDesc &d, int rs, int &col, unsigned short &val) {
+        const int j0 = __shfl_sync(full, rs, 0), j1 = __shfl_sync(full, rs, d.nrows & 31);
+        col = 0;
+        val = 0;
+        if (d.nrows > 0 && j0 + lane < j1) {
+            const CcJob &a = b.job[d.job];
+            col = __ldg(a.p_col + j0 + lane);
+            val = __half_as_ushort(a.p_val[j0 + lane]);
+        }
+    };
+
+    ItemDesc d0 = load_desc(b, item), d1 = load_desc(b, item + n_warps), d2 = load_desc(b, item + 2 * n_warps);
+    int rs0, out0, rs1, out1, col0;
+    unsigned short val0;
+    load_rows(d0, rs0, out0);
+    load_rows(d1, rs1, out1);
+    load_nz(d0, rs0, col0, val0);
+
+    while (d0.nrows > 0) {
+        int col1;
+        unsigned short val1;
+        load_nz(d1, rs1, col1, val1);
+        int rs2, out2;
+        load_rows(d2, rs2, out2);
+        const ItemDesc d3 = load_desc(b, item + 3 * n_warps);
+
+        const CcJob &a = b.job[d0.job];
+        const int R = d0.nrows;
+        const int j0 = __shfl_sync(full, rs0, 0), j1 = __shfl_sync(full, rs0, R);
+        const int Z = j1 - j0;
+        const int G = R > 16 ? 2 : 1; // 16-row groups
+        const bool keep = (a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) != 0;
+        // local row of this lane's nonzero (rows of an item are consecutive)
+        int rz = 0;
+        for (int r = 1; r < R; r++) rz += (lane >= __shfl_sync(full, rs0, r) - j0) ? 1 : 0;
+
+        for (int n0 = 0; n0 < a.N; n0 += kMmaSliceCols) {
+            float acc[2][8][4];
+#pragma unroll
+            for (int gg = 0; gg < 2; gg++)
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[gg][t][q] = 0.f;
+            for (int kb = 0; kb < Z; kb += 32) {
+                int col = col0, zr = rz;
+                unsigned short val = val0;
+                if (kb > 0) { // a row longer than 32 nonzeros: its next 32
+                    col = 0;
+                    val = 0;
+                    zr = 0;
+                    if (kb + lane < Z) {
+                        col = __ldg(a.p_col + j0 + kb + lane);
+                        val = __half_as_ushort(a.p_val[j0 + kb + lane]);
+                    }
+                }
+                const int zc = min(32, Z - kb);
+                // stage B rows z = 4 i + lane / 8, 16-byte chunk lane % 8 of the slice
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const int z = 4 * i + (lane >> 3), q = lane & 7;
+                    const int cz = __shfl_sync(full, col, z);
+                    uint4 v = make_uint4(0, 0, 0, 0);
+                    if (z < zc && n0 + 8 * q < a.N)
+                        v = __ldg(reinterpret_cast<const uint4 *>(a.B + (size_t)cz * a.ldb + n0 + 8 * q));
+                    *reinterpret_cast<uint4 *>(ws + z * 128 + ((q ^ (z & 7)) << 4)) = v;
+                }
+                __syncwarp();
+#pragma unroll
+                for (int ks = 0; ks < 2; ks++) {
+                    if (16 * ks >= zc)
+                        break; // uniform
+                    // A fragments: k = 16 ks + 2 c4 + {0, 1} (+ 8); rows 16 gg + g (+ 8)
+                    uint32_t af[2][4];
+                    int kk[4] = {16 * ks + 2 * c4, 16 * ks + 2 * c4 + 1, 16 * ks + 2 * c4 + 8, 16 * ks + 2 * c4 + 9};
+                    int rk[4];
+                    unsigned short vk[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        rk[u] = __shfl_sync(full, zr, kk[u]);
+                        vk[u] = (unsigned short)__shfl_sync(full, (int)val, kk[u]);
+                        if (kk[u] >= zc) rk[u] = -1;
+                    }
+#pragma unroll
+                    for (int gg = 0; gg < 2; gg++) {
+                        const int r_lo = 16 * gg + g, r_hi = r_lo + 8;
+                        auto pk = [&](int u0, int u1, int row) -> uint32_t {
+                            const uint32_t lo = rk[u0] == row ? vk[u0] : 0u;
+                            const uint32_t hi = rk[u1] == row ? vk[u1] : 0u;
+                            return lo | (hi << 16);
+                        };
+                        af[gg][0] = pk(0, 1, r_lo);
+                        af[gg][1] = pk(0, 1, r_hi);
+                        af[gg][2] = pk(2, 3, r_lo);
+                        af[gg][3] = pk(2, 3, r_hi);
+                    }
+#pragma unroll
+                    for (int p = 0; p < 4; p++) {
+                        const int mi = lane >> 3;
+                        const int krow = 16 * ks + (lane & 7) + (mi & 1) * 8;
+                        const int nch = 2 * p + (mi >> 1);
+                        uint32_t bf[4];
+                        ldmatrix_x4_trans(ws_addr + krow * 128 + ((nch ^ (krow & 7)) << 4), bf);
+                        mma_16816(acc[0][2 * p], af[0], bf[0], bf[1]);
+                        mma_16816(acc[0][2 * p + 1], af[0], bf[2], bf[3]);
+                        if (G == 2) {
+                            mma_16816(acc[1][2 * p], af[1], bf[0], bf[1]);
+                            mma_16816(acc[1][2 * p + 1], af[1], bf[2], bf[3]);
+                        }
+                    }
+                }
+            }
+            // ---- epilogue of the slice, per 16-row group, through shared memory
+#pragma unroll
+            for (int gg = 0; gg < 2; gg++) {
+                if (gg >= G)
+                    break;
+                __syncwarp();
+#pragma unroll
+                for (int t = 0; t < 8; t++) {
+                    *reinterpret_cast<float2 *>(acc_s + g * kMmaAccStride + 8 * t + 2 * c4) =
+                        make_float2(acc[gg][t][0], acc[gg][t][1]);
+                    *reinterpret_cast<float2 *>(acc_s + (g + 8) * kMmaAccStride + 8 * t + 2 * c4) =
+                        make_float2(acc[gg][t][2], acc[gg][t][3]);
+                }
+                __syncwarp();
+                const int rows = min(16, R - 16 * gg);
+                for (int i = 0; 4 * i < rows; i++) {
+                    const int rl = 4 * i + (lane >> 3); // row within the group
+                    const int r = 16 * gg + rl;          // row within the item
+                    const int orow = __shfl_sync(full, out0, r & 31);
+                    const int rstart = __shfl_sync(full, rs0, r & 31), rend = __shfl_sync(full, rs0, (r + 1) & 31);
+                    const int n = n0 + (lane & 7) * 8;
+                    if (rl < rows && n < a.N && !(keep && rstart == rend)) {
+                        const float4 v0 = *reinterpret_cast<const float4 *>(acc_s + rl * kMmaAccStride + (lane & 7) * 8);
+                        const float4 v1 =
+                            *reinterpret_cast<const float4 *>(acc_s + rl * kMmaAccStride + (lane & 7) * 8 + 4);
+                        const float v[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+                        OutT *cp = reinterpret_cast<OutT *>(a.C) + (size_t)orow * a.ldc + n;
+                        float o[8];
+                        if (a.beta != 0.f) {
+                            float old[8];
+                            load_out<8>(cp, old);
+#pragma unroll
+                            for (int q = 0; q < 8; q++) o[q] = fmaf(a.alpha, v[q], a.beta * old[q]);
+                        } else {
+#pragma unroll
+                            for (int q = 0; q < 8; q++) o[q] = a.alpha * v[q];
+                        }
+                        store_out<8>(cp, o);
+                    }
+                }
+            }
+        }
+
+        d0 = d1; rs0 = rs1; out0 = out1; col0 = col1; val0 = val1;
+        d1 = d2; rs1 = rs2; out1 = out2;
+        d2 = d3;
+        item += n_warps;
+    }
+}
+
 // Persistent grid of the stream kernel: enough warps for every item, at most
 // the resident blocks of all SMs.
+// beside_regs > 0: the launch directly follows a tensor-core launch whose
+// one block per SM holds that many registers. It is issued as a programmatic
+// dependent of that launch (which triggers at entry), so its blocks start as
+// soon as the tensor-core blocks are resident, and its grid is cut to the
+// blocks that fit beside them (a block that waited for the tensor-core kernel
+// to end would start its fixed share of the items late). The kernel reads
+// nothing the tensor-core kernel writes, so it never waits on it.
 template <typename OutT, int W, bool F8>
-int launch_stream_group(const CcBatch &b, cudaStream_t s)
+int launch_stream_group(const CcBatch &b, int beside_regs, cudaStream_t s)
+{
+    const int total = b.item_start[b.n_jobs];
+    if (b.n_jobs == 0 || total == 0)
+        return TCA_OK;
+    static int per_sm = 0, regs = 0;
+    if (per_sm == 0) {
+        int n = 0;
+        TCA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spmm_cc_stream_kernel<OutT, W, F8>, 256, 0));
+        TCA_TRY(block_regs((const void *)spmm_cc_stream_kernel<OutT, W, F8>, 256, &regs));
+        per_sm = n > 0 ? n : 1;
+    }
+    const int fit = beside_regs > 0 ? std::max(1, std::min(per_sm, (kSmRegs - beside_regs) / regs)) : per_sm;
+    const int grid = std::min((total + 7) / 8, kSMs * fit);
+    if (beside_regs > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(256);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        TCA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmm_cc_stream_kernel<OutT, W, F8>, b));
+        return TCA_OK;
+    }
+    spmm_cc_stream_kernel<OutT, W, F8><<<grid, 256, 0, s>>>(b);
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
+template <typename OutT>
+int launch_mma_group(const CcBatch &b, cudaStream_t s)
 {
     const int total = b.item_start[b.n_jobs];
     if (b.n_jobs == 0 || total == 0)
@@ -696,11 +973,11 @@ int launch_stream_group(const CcBatch &b, cudaStream_t s)
     static int per_sm = 0;
     if (per_sm == 0) {
         int n = 0;
-        TCA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spmm_cc_stream_kernel<OutT, W, F8>, 256, 0));
+        TCA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spmm_cc_mma_kernel<OutT>, kMmaWarps * 32, 0));
         per_sm = n > 0 ? n : 1;
     }
-    const int grid = std::min((total + 7) / 8, kSMs * per_sm);
-    spmm_cc_stream_kernel<OutT, W, F8><<<grid, 256, 0, s>>>(b);
+    const int grid = std::min((total + kMmaWarps - 1) / kMmaWarps, kSMs * per_sm);
+    spmm_cc_mma_kernel<OutT><<<grid, kMmaWarps * 32, 0, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
 }
@@ -709,29 +986,31 @@ int launch_stream_group(const CcBatch &b, cudaStream_t s)
 inline int pick_w(int N) { return N > 128 ? 8 : N > 64 ? 4 : 2; }
 
 template <typename OutT, bool F8>
-int launch_stream_w(const CcBatch &b, int w, cudaStream_t s)
+int launch_stream_w(const CcBatch &b, int w, int beside_regs, cudaStream_t s)
 {
     switch (w) {
-    case 2: return launch_stream_group<OutT, 2, F8>(b, s);
-    case 4: return launch_stream_group<OutT, 4, F8>(b, s);
-    default: return launch_stream_group<OutT, 8, F8>(b, s);
+    case 2: return launch_stream_group<OutT, 2, F8>(b, beside_regs, s);
+    case 4: return launch_stream_group<OutT, 4, F8>(b, beside_regs, s);
+    default: return launch_stream_group<OutT, 8, F8>(b, beside_regs, s);
     }
 }
 
 template <typename OutT>
-int launch_cc_typed(const CcBatch &b, int w, bool vec, bool f8, cudaStream_t s)
+int launch_cc_typed(const CcBatch &b, int w, bool vec, bool f8, int beside_regs, cudaStream_t s)
 {
     if (!vec) return launch_cc_group<OutT, 32, false>(b, s);
-    return f8 ? launch_stream_w<OutT, true>(b, w, s) : launch_stream_w<OutT, false>(b, w, s);
+    if (w == kCcMma) return launch_mma_group<OutT>(b, s);
+    return f8 ? launch_stream_w<OutT, true>(b, w, beside_regs, s) : launch_stream_w<OutT, false>(b, w, beside_regs, s);
 }
 
 } // namespace
 
 int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s, LaunchList *defer)
+                   cudaStream_t s, LaunchList *defer, int beside_regs)
 {
     // groups: (columns per lane, vectorised, E4M3) -- stream kernel with 2/4/8 columns, scalar items
-    const int kinds[7][3] = {{2, 1, 0}, {4, 1, 0}, {8, 1, 0}, {32, 0, 0}, {2, 1, 1}, {4, 1, 1}, {8, 1, 1}};
+    // and the FP16 tensor-core item kernel (kCcMma)
+    const int kinds[8][3] = {{2, 1, 0}, {4, 1, 0}, {8, 1, 0}, {kCcMma, 1, 0}, {32, 0, 0}, {2, 1, 1}, {4, 1, 1}, {8, 1, 1}};
     for (const auto &kd : kinds) {
         CcBatch b;
         b.n_jobs = 0;
@@ -742,9 +1021,9 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
                 return TCA_OK;
             const int w = kd[0];
             const bool vec = kd[1] != 0, f8 = kd[2] != 0;
-            auto run = [c_dtype, w, vec, f8](const CcBatch &bb, cudaStream_t st) {
-                return (c_dtype == TCA_DTYPE_F16) ? launch_cc_typed<__half>(bb, w, vec, f8, st)
-                                                  : launch_cc_typed<float>(bb, w, vec, f8, st);
+            auto run = [c_dtype, w, vec, f8, beside_regs](const CcBatch &bb, cudaStream_t st) {
+                return (c_dtype == TCA_DTYPE_F16) ? launch_cc_typed<__half>(bb, w, vec, f8, beside_regs, st)
+                                                  : launch_cc_typed<float>(bb, w, vec, f8, beside_regs, st);
             };
             int status = TCA_OK;
             if (defer) {
@@ -764,7 +1043,12 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
                 continue;
             // E4M3 jobs always qualify (B is the library's own aligned copy; C was checked)
             const bool vec = sj.f8 || vec_ok(sj.B, sj.ldb, sj.N, sj.C, sj.ldc, c_dtype);
-            const int lpr = vec ? (sj.cc_w == 2 || sj.cc_w == 4 || sj.cc_w == 8 ? sj.cc_w : pick_w(sj.N)) : 32;
+            int lpr = 32;
+            if (vec) {
+                lpr = (sj.cc_w == 2 || sj.cc_w == 4 || sj.cc_w == 8) ? sj.cc_w : pick_w(sj.N);
+                if (sj.cc_w == kCcMma && !sj.f8)
+                    lpr = kCcMma;
+            }
             if (lpr != kd[0] || (vec ? 1 : 0) != kd[1] || (sj.f8 ? 1 : 0) != kd[2])
                 continue;
             CcJob &a = b.job[b.n_jobs];

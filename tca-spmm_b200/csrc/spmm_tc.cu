@@ -228,6 +228,11 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     constexpr int kScatterGroups = S % 2 == 0 ? 2 : 1; // two groups need an even ring (see the scatter role)
     constexpr int kGroupThreads = kScatterThreads / kScatterGroups;
 
+    // A CUDA-core launch that follows on the stream as a programmatic
+    // dependent may start as soon as every block of this grid is resident: it
+    // reads nothing this kernel writes (the two paths own disjoint rows of C).
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = batch.item_start[batch.n_jobs];
     const int n_items = blockIdx.x < total ? min(kMaxCtaItems, (total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1) : 0;
@@ -625,6 +630,36 @@ int pick_tc_tile(int n_tc, int N, bool batched, bool f8)
         while (NT > lo && (long long)n_tc * ((N + NT - 1) / NT) < kSMs)
             NT /= 2;
     return NT;
+}
+
+int tc_block_regs(bool f8, int *regs)
+{
+    static int worst[2] = {0, 0};
+    if (worst[f8] == 0) {
+        const void *f16_fns[] = {
+            (const void *)spmm_tc_kernel<64, __half, false>, (const void *)spmm_tc_kernel<128, __half, false>,
+            (const void *)spmm_tc_kernel<256, __half, false>, (const void *)spmm_tc_kernel<64, float, false>,
+            (const void *)spmm_tc_kernel<128, float, false>, (const void *)spmm_tc_kernel<256, float, false>};
+        const void *f8_fns[] = {
+            (const void *)spmm_tc_kernel<128, __half, true>, (const void *)spmm_tc_kernel<256, __half, true>,
+            (const void *)spmm_tc_kernel<128, float, true>, (const void *)spmm_tc_kernel<256, float, true>};
+        int w = 0;
+        for (const void *f : f16_fns) {
+            if (f8) break;
+            int r = 0;
+            TCA_TRY(block_regs(f, kThreads, &r));
+            w = std::max(w, r);
+        }
+        for (const void *f : f8_fns) {
+            if (!f8) break;
+            int r = 0;
+            TCA_TRY(block_regs(f, kThreads, &r));
+            w = std::max(w, r);
+        }
+        worst[f8] = w;
+    }
+    *regs = worst[f8];
+    return TCA_OK;
 }
 
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,

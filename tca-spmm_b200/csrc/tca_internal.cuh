@@ -35,6 +35,19 @@ void clear_error();
 
 inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+constexpr int kSmRegs = 65536; // registers of one SM
+
+// Registers that one block of kernel `fn` with `threads` threads holds on an
+// SM: per warp, its registers per thread x 32 rounded up to the allocation
+// unit of 256.
+inline int block_regs(const void *fn, int threads, int *out)
+{
+    cudaFuncAttributes a;
+    TCA_CUDA_TRY(cudaFuncGetAttributes(&a, fn));
+    *out = ((a.numRegs * 32 + 255) / 256) * 256 * ((threads + 31) / 32);
+    return TCA_OK;
+}
+
 // Device memory of the library (api.cu): stream-ordered allocations from a
 // per-device memory pool that keeps freed memory for reuse (plan builds and
 // host-buffer calls allocate and free dozens of arrays per call; plain

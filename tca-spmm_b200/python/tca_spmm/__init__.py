@@ -348,14 +348,15 @@ class Plan:
 
 
 def spmm_batched(plans, Bs, outs, alpha=1.0, beta=0.0, keep_empty_rows=False, n_tile=0, events=None,
-                 stream=None):
+                 stream=None, cc_cols=0):
     """Forwards of many plans in a few launches (tca_spmm_batched). `outs`
-    must all have the same dtype (float16 or float32)."""
+    must all have the same dtype (float16 or float32). cc_cols picks the
+    CUDA-core kernel of every item (CC_COLS_*; 0 = by N)."""
     n = len(plans)
     arr = (BatchItem * max(n, 1))()
     for i, (p, B, C) in enumerate(zip(plans, Bs, outs)):
         N, _ = _prepare_dense(B, C, p.M, C.dtype)
-        arr[i] = BatchItem(p.handle, _ptr(B), B.stride(0), N, _ptr(C), C.stride(0), n_tile)
+        arr[i] = BatchItem(p.handle, _ptr(B), B.stride(0), N, _ptr(C), C.stride(0), n_tile, cc_cols)
     code = _out_code(outs[0].dtype) if n else DTYPE_F16
     ev = None
     if events is not None:
@@ -384,6 +385,9 @@ def spmm_fp8_batched(plans, Bs, outs, alpha=1.0, beta=0.0, keep_empty_rows=False
 
 
 PRECISION_F16, PRECISION_E4M3 = 0, 1
+# cc_cols values: the CUDA-core stream kernel with 2, 4 or 8 output columns
+# per lane, or the FP16 tensor-core item kernel (mma.sync)
+CC_COLS_2, CC_COLS_4, CC_COLS_8, CC_COLS_MMA = 2, 4, 8, 16
 _PRECISIONS = {"f16": PRECISION_F16, "fp16": PRECISION_F16, "e4m3": PRECISION_E4M3, "fp8": PRECISION_E4M3}
 
 

@@ -76,7 +76,7 @@ def test_autotuned_graph(layers):
     tuned = tca_spmm.autotune(plans, Bs, outs, reps=3)
     assert len(tuned) == len(plans)
     for (nt, w), c in zip(tuned, ls):
-        assert nt in (64, 128, 256) and w in (2, 4, 8)
+        assert nt in (64, 128, 256) and w in (2, 4, 8, tca_spmm.CC_COLS_MMA)
     g = tca_spmm.BatchGraph(plans, Bs, outs, n_tiles=[t[0] for t in tuned], cc_cols=[t[1] for t in tuned])
     for C in outs:
         C.zero_()
