@@ -175,7 +175,8 @@ typedef struct tca_batch_item {
     void *d_C;
     int ldc;
     int n_tile;   /* tensor-core N-slice width: 64, 128, 256 (E4M3: 128, 256); 0 = by N */
-    int cc_cols;  /* CUDA-core output columns per lane: 2, 4, 8; 0 = by N */
+    int cc_cols;  /* CUDA-core output columns per lane: 2, 4, 8; 16 = the FP16
+                     mma.sync item kernel (E4M3 items: by N); 0 = by N */
 } tca_batch_item_t;
 
 /* Forwards of many plans (layers of different shapes and sparsity) in a

@@ -425,8 +425,14 @@ __device__ __forceinline__ ItemDesc load_desc(const CcBatch &b, int item)
 {
     ItemDesc d{0, 0, 0};
     if (item < b.item_start[b.n_jobs]) {
-        int j = 0;
-        while (j + 1 < b.n_jobs && b.item_start[j + 1] <= item) j++;
+        int j = 0, hi = b.n_jobs - 1; // the last job whose first item is <= item
+        while (j < hi) {
+            const int mid = (j + hi + 1) >> 1;
+            if (b.item_start[mid] <= item)
+                j = mid;
+            else
+                hi = mid - 1;
+        }
         const int2 it = __ldg(b.job[j].items + (item - b.item_start[j]));
         d.job = j;
         d.r0 = it.x;
@@ -440,6 +446,52 @@ template <int W, bool F8> struct BVec { using T = typename HalfVec<W>::T; };
 template <> struct BVec<8, true> { using T = uint2; };
 template <> struct BVec<4, true> { using T = unsigned; };
 template <> struct BVec<2, true> { using T = unsigned short; };
+
+// One output row's W columns: t = acc (E4M3: x row scale sa x column scales
+// sb), then alpha t + beta C.
+template <typename OutT, int W, bool F8>
+__device__ __forceinline__ void store_row(const CcJob &a, int orow, int n0, const float *acc, float sa,
+                                          const float *sb)
+{
+    OutT *cp = reinterpret_cast<OutT *>(a.C) + (size_t)orow * a.ldc + n0;
+    float t[W], o[W];
+#pragma unroll
+    for (int i = 0; i < W; i++) {
+        if constexpr (F8)
+            t[i] = acc[i] * (sa * sb[i]);
+        else
+            t[i] = acc[i];
+    }
+    if (a.beta != 0.f) {
+        float old[W];
+        load_out<W>(cp, old);
+#pragma unroll
+        for (int i = 0; i < W; i++) o[i] = fmaf(a.alpha, t[i], a.beta * old[i]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < W; i++) o[i] = a.alpha * t[i];
+    }
+    store_out<W>(cp, o);
+}
+
+// acc[i] = v * b[i] + acc[i] over one B vector (E4M3 pairs unpacked to FP16).
+template <int W, bool F8, typename V>
+__device__ __forceinline__ void fma_vec(float *acc, unsigned short v, const V &bv)
+{
+    if constexpr (F8) {
+        const __nv_fp8x2_storage_t *q = reinterpret_cast<const __nv_fp8x2_storage_t *>(&bv);
+#pragma unroll
+        for (int i = 0; i < W / 2; i++) {
+            const __half2_raw h = __nv_cvt_fp8x2_to_halfraw2(q[i], __NV_E4M3);
+            acc[2 * i] = fma_f16_f32(v, h.x, acc[2 * i]);
+            acc[2 * i + 1] = fma_f16_f32(v, h.y, acc[2 * i + 1]);
+        }
+    } else {
+        const unsigned short *h = reinterpret_cast<const unsigned short *>(&bv);
+#pragma unroll
+        for (int i = 0; i < W; i++) acc[i] = fma_f16_f32(v, h[i], acc[i]);
+    }
+}
 
 // F8: values and B are E4M3 (every E4M3 value is an FP16 value, so the
 // products are formed exactly by the same mixed-precision FMA); the flush
@@ -519,7 +571,52 @@ __global__ void __launch_bounds__(256, 3) spmm_cc_stream_kernel(const __grid_con
         const int nrows = d0.nrows;
         const int j0 = __shfl_sync(full, rs0, 0), j1 = __shfl_sync(full, rs0, nrows);
         const bool keep = (a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) != 0;
-        for (int nb = 0; nb < a.N; nb += 32 * W) {
+        // Items whose rows hold one nonzero each (the short-row tails of skewed
+        // matrices): C[row] = alpha v B[col] (+ beta C[row]) row by row, with U
+        // rows' B vectors in flight and no row-boundary tracking.
+        const int rs_next = __shfl_down_sync(full, rs0, 1);
+        const bool singles = __all_sync(full, lane >= nrows || rs_next - rs0 == 1);
+        for (int nb = 0; singles && nb < a.N; nb += 32 * W) {
+            const int n0 = nb + lane * W;
+            const bool active = n0 < a.N;
+            const uint8_t *Bn = F8 ? a.Bq + (active ? n0 : 0)
+                                   : reinterpret_cast<const uint8_t *>(a.B + (active ? n0 : 0));
+            const size_t brow = F8 ? (size_t)a.ldq : (size_t)a.ldb * 2; // bytes per B row
+            float sb[F8 ? W : 1];
+            if constexpr (F8) {
+#pragma unroll
+                for (int i = 0; i < W; i++) sb[i] = active ? __ldg(a.col_scale + n0 + i) : 0.f;
+            }
+            for (int t = 0; t < nrows; t += U) {
+                V bv[U];
+                unsigned short av[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int r = (t + u) & 31;
+                    const int cu = __shfl_sync(full, col0, r);
+                    av[u] = (unsigned short)__shfl_sync(full, (int)val0, r);
+                    bv[u] = V{};
+                    if (active && t + u < nrows)
+                        bv[u] = __ldg(reinterpret_cast<const V *>(Bn + (size_t)cu * brow));
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int r = (t + u) & 31;
+                    const int orow = __shfl_sync(full, out0, r);
+                    float sa = 1.f;
+                    if constexpr (F8)
+                        sa = __shfl_sync(full, sc0, r);
+                    if (active && t + u < nrows) {
+                        float acc[W];
+#pragma unroll
+                        for (int i = 0; i < W; i++) acc[i] = 0.f;
+                        fma_vec<W, F8>(acc, av[u], bv[u]);
+                        store_row<OutT, W, F8>(a, orow, n0, acc, sa, sb);
+                    }
+                }
+            }
+        }
+        for (int nb = 0; !singles && nb < a.N; nb += 32 * W) {
             const int n0 = nb + lane * W;
             const bool active = n0 < a.N;
             const uint8_t *Bn = F8 ? a.Bq + (active ? n0 : 0)
@@ -541,27 +638,8 @@ __global__ void __launch_bounds__(256, 3) spmm_cc_stream_kernel(const __grid_con
                 float sa = 1.f;
                 if constexpr (F8)
                     sa = __shfl_sync(full, sc0, cr);
-                if (active && !(keep && rstart == ce)) {
-                    OutT *cp = reinterpret_cast<OutT *>(a.C) + (size_t)orow * a.ldc + n0;
-                    float t[W], o[W];
-#pragma unroll
-                    for (int i = 0; i < W; i++) {
-                        if constexpr (F8)
-                            t[i] = acc[i] * (sa * sb[i]);
-                        else
-                            t[i] = acc[i];
-                    }
-                    if (a.beta != 0.f) {
-                        float old[W];
-                        load_out<W>(cp, old);
-#pragma unroll
-                        for (int i = 0; i < W; i++) o[i] = fmaf(a.alpha, t[i], a.beta * old[i]);
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < W; i++) o[i] = a.alpha * t[i];
-                    }
-                    store_out<W>(cp, o);
-                }
+                if (active && !(keep && rstart == ce))
+                    store_row<OutT, W, F8>(a, orow, n0, acc, sa, sb);
 #pragma unroll
                 for (int i = 0; i < W; i++) acc[i] = 0.f;
                 cr++;
@@ -595,19 +673,7 @@ __global__ void __launch_bounds__(256, 3) spmm_cc_stream_kernel(const __grid_con
                     for (int u = 0; u < U; u++) {
                         if (t + u < m) { // uniform across the warp
                             while (base + t + u >= ce) flush();
-                            if constexpr (F8) {
-                                const __nv_fp8x2_storage_t *q = reinterpret_cast<const __nv_fp8x2_storage_t *>(&bv[u]);
-#pragma unroll
-                                for (int i = 0; i < W / 2; i++) {
-                                    const __half2_raw h = __nv_cvt_fp8x2_to_halfraw2(q[i], __NV_E4M3);
-                                    acc[2 * i] = fma_f16_f32(av[u], h.x, acc[2 * i]);
-                                    acc[2 * i + 1] = fma_f16_f32(av[u], h.y, acc[2 * i + 1]);
-                                }
-                            } else {
-                                const unsigned short *h = reinterpret_cast<const unsigned short *>(&bv[u]);
-#pragma unroll
-                                for (int i = 0; i < W; i++) acc[i] = fma_f16_f32(av[u], h[i], acc[i]);
-                            }
+                            fma_vec<W, F8>(acc, av[u], bv[u]);
                         }
                     }
                 }
