@@ -71,6 +71,14 @@ TCA_API void perform_cuSPARSE_SpMM(half *A, half *B, float *C, int M, int N, int
 TCA_API void perform_cuSPARSE_BlockSpMM(half *A, half *B, float *C, int M, int N, int K, int num_iter,
                                         int ell_block_size, double *elapsed = NULL);
 
+/* src/spmm_cusparse.cuh, src/spmm_cusparse.cu:2 -- cuSPARSELt 2:4 comparator
+ * on a dense A: cuSPARSELt prunes A to the 2:4 pattern along its rows (STRIP),
+ * compresses it and multiplies with B: FP16 A/B, FP32 compute, FP16 result
+ * returned as FP32 C, num_iter timed calls. A different product (A pruned);
+ * cuSPARSELt is loaded at the first call (an error is reported without it). */
+TCA_API void perform_cuSPARSELT_24sparsity(half *A, half *B, float *C, int M, int N, int K, int num_iter,
+                                           double *elapsed = NULL);
+
 /* src/gemm_cublas.cuh:12, src/gemm_cublas.cu:3 -- dense cuBLAS GemmEx gold:
  * FP16 A/B, FP32 C and compute, 5 warm-up then n_iter timed calls. */
 TCA_API void perform_GemmEx(half *A, half *B, float *C, int M, int N, int K, int n_iter,

@@ -311,6 +311,7 @@ def ref() -> ctypes.CDLL:
         R.ref_cusparse_blockspmm.argtypes = [_P, _P, _P, _I, _I, _I, _I, _I, D]
         R.ref_cusparse_blockspmm.restype = None
         R.ref_gemmex.argtypes = [_P, _P, _P, _I, _I, _I, _I, D]; R.ref_gemmex.restype = None
+        R.ref_cusparselt_24.argtypes = [_P, _P, _P, _I, _I, _I, _I, D]; R.ref_cusparselt_24.restype = None
         _ref = R
     return _ref
 
@@ -418,6 +419,33 @@ def ref_cusparse_blockspmm(A, B, bs, C=None, n_iter=1):
     ref().ref_cusparse_blockspmm(Ab.ctypes.data, Bb.ctypes.data, out.ctypes.data, M, N, K, n_iter, bs,
                                  ctypes.byref(ms))
     return out, ms.value
+
+
+def ref_cusparselt_24(A, B, n_iter=1):
+    """The reference's cuSPARSELt 2:4 comparator: (C, ms) for A pruned by
+    cuSPARSELt times B."""
+    Ab, Bb = f16_bits(A), f16_bits(B)
+    M, K = Ab.shape
+    N = Bb.shape[1]
+    out = np.zeros((M, N), np.float32)
+    ms = ctypes.c_double(-1.0)
+    ref().ref_cusparselt_24(Ab.ctypes.data, Bb.ctypes.data, out.ctypes.data, M, N, K, n_iter, ctypes.byref(ms))
+    return out, ms.value
+
+
+def prune_24_rows(A):
+    """2:4 pruning along the rows of a dense matrix (K a multiple of 4): in
+    every group of four consecutive elements of a row the two of largest
+    magnitude stay, the other two become zero (cuSPARSELt's STRIP pruning,
+    src/spmm_cusparse.cu:83; ties between equal magnitudes are not resolved
+    here -- callers use data without them)."""
+    A = np.asarray(A)
+    M, K = A.shape
+    g = A.reshape(M, K // 4, 4)
+    order = np.argsort(-np.abs(g.astype(np.float32)), axis=2, kind="stable")
+    keep = np.zeros(g.shape, bool)
+    np.put_along_axis(keep, order[:, :, :2], True, axis=2)
+    return np.where(keep, g, np.zeros_like(g)).reshape(M, K)
 
 
 def ref_gemmex(A, B, C=None, n_iter=1):

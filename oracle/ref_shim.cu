@@ -159,6 +159,14 @@ void ref_cusparse_blockspmm(const uint16_t *A, const uint16_t *B, float *C, int 
                                reinterpret_cast<half *>(const_cast<uint16_t *>(B)), C, M, N, K, n_iter, bs, elapsed);
 }
 
+// perform_cuSPARSELT_24sparsity (src/spmm_cusparse.cu:2): 2:4 comparator (A pruned).
+void ref_cusparselt_24(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K, int n_iter,
+                       double *elapsed)
+{
+    perform_cuSPARSELT_24sparsity(reinterpret_cast<half *>(const_cast<uint16_t *>(A)),
+                                  reinterpret_cast<half *>(const_cast<uint16_t *>(B)), C, M, N, K, n_iter, elapsed);
+}
+
 // perform_GemmEx (src/gemm_cublas.cu:3): the reference test's dense gold.
 void ref_gemmex(const uint16_t *A, const uint16_t *B, float *C, int M, int N, int K, int n_iter, double *elapsed)
 {
