@@ -17,6 +17,9 @@ L2 and every problem is read from HBM.
              work it does per launch / its mean CUDA-event duration
   cpu_baseline  the oracle's OpenMP FP32 CSR x dense on the host cores, one
              problem, repeated for a bounded time
+  fp8, batching, fwd_bwd  the E4M3 step, the 24-layer batch (graph vs
+             sequential) and the differentiation config (forward vs forward +
+             SDDMM + transpose SpMM, gradient errors vs FP64)
 
 --impl reference runs the reference's own TCA kernel (our_spmm_balanced,
 built from the reference sources into oracle/_ref) through its host API on
@@ -348,6 +351,7 @@ def run_ours(args, world, rank):
         "e2e": e2e,
         "fp8": fp8,
         "batching": batching_leg(args, world),
+        "fwd_bwd": fwd_bwd_leg(args, rank == 0 and not args.no_cpu),
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
     }
@@ -417,6 +421,63 @@ def batching_leg(args, world):
             "graph_us": round(t_graph, 2), "sequential_us": round(t_seq, 2),
             "speedup": round(t_seq / t_graph, 3), "graph_gflops": round(flops / (t_graph * 1e-6) / 1e9, 1),
             "tuned": [list(t) for t in tuned]}
+
+
+def fwd_bwd_leg(args, check):
+    """The differentiation config (A 2048 x 512 at 90 %, B 512 x 4096, dY
+    2048 x 4096): forward alone vs forward + backward (dA = SDDMM(dY, B) on
+    A's pattern, dB = A^T dY), device time per pass (CUDA events, median of
+    runs), and with `check` the gradients' error against FP64."""
+    import torch
+    import tca_spmm
+    from tca_spmm import gen
+    dev = torch.device("cuda", torch.cuda.current_device())
+    c = gen.diff()
+    rp, ci, v = (torch.from_numpy(x.copy()).to(dev) for x in (c["row_ptr"], c["col"], c["vals"]))
+    B = torch.from_numpy(c["B"]).to(dev)
+    dY = torch.from_numpy(c["dY"]).to(dev)
+    plan = tca_spmm.Plan(rp, ci, v, c["K"])
+    Y = torch.empty((c["M"], c["N"]), dtype=torch.float16, device=dev)
+    dA = torch.empty(c["col"].size, dtype=torch.float32, device=dev)
+    dB = torch.empty((c["K"], c["N"]), dtype=torch.float32, device=dev)
+
+    def fwd():
+        plan.spmm(B, out=Y)
+
+    def fwd_bwd():
+        plan.spmm(B, out=Y)
+        plan.sddmm(dY, B, out=dA)
+        plan.spmm_t(dY, out=dB)
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b) * 1e3)
+        return float(np.median(ts))
+
+    t_f, t_fb = timed(fwd), timed(fwd_bwd)
+    flops = 2.0 * c["col"].size * c["N"]
+    out = {"workload": "A 2048x512 90% (uniform rows), B 512x4096, dY 2048x4096, FP16 in, FP32 dA/dB",
+           "fwd_us": round(t_f, 2), "fwd_bwd_us": round(t_fb, 2), "fwd_bwd_over_fwd": round(t_fb / t_f, 3),
+           "fwd_gflops": round(flops / (t_f * 1e-6) / 1e9, 1),
+           "fwd_bwd_gflops": round(3 * flops / (t_fb * 1e-6) / 1e9, 1)}
+    if check:
+        rows = np.repeat(np.arange(c["M"]), np.diff(c["row_ptr"]))
+        B64, Y64 = c["B"].astype(np.float64), c["dY"].astype(np.float64)
+        dA64 = np.einsum("jn,jn->j", Y64[rows], B64[c["col"]])
+        dB64 = np.zeros_like(B64)
+        np.add.at(dB64, c["col"], c["vals"].astype(np.float64)[:, None] * Y64[rows])
+        out["dA_rel_err_vs_f64"] = float(f"{np.linalg.norm(dA.cpu().numpy() - dA64) / np.linalg.norm(dA64):.3e}")
+        out["dB_rel_err_vs_f64"] = float(f"{np.linalg.norm(dB.cpu().numpy() - dB64) / np.linalg.norm(dB64):.3e}")
+    return out
 
 
 def run_reference(args, world, rank):

@@ -81,3 +81,62 @@ def _rank(rank, world, port, seed):
 def test_two_gloo_ranks_gather_rows_and_sum_grad_b():
     import torch.multiprocessing as mp
     mp.spawn(_rank, args=(2, _free_port(), 123), nprocs=2, join=True)
+
+
+def test_partition_cols_covers_and_aligns():
+    for N, n in [(256, 2), (264, 4), (8, 3), (100, 3), (1, 2)]:
+        c = shard.partition_cols(N, n)
+        assert c[0] == 0 and c[-1] == N and (np.diff(c) >= 0).all()
+        assert all(x % 8 == 0 for x in c[:-1])
+        w = np.diff(c)
+        assert w.max() - w.min() <= 8 or N < 8 * n
+
+
+def test_assign_layers_lpt():
+    costs = [7, 3, 9, 1, 4, 4, 8]
+    out = shard.assign_layers_lpt(costs, 3)
+    assert sorted(i for r in out for i in r) == list(range(len(costs)))
+    # 9 -> r0, 8 -> r1, 7 -> r2, 4 (#4) -> r2, 4 (#5) -> r1, 3 -> r0, 1 -> r2
+    assert out == [[1, 2], [5, 6], [0, 3, 4]]
+    assert [sum(costs[i] for i in r) for r in out] == [12, 12, 12]
+    assert shard.assign_layers_lpt([5, 5], 4) == [[0], [1], [], []]
+    assert shard.assign_layers_lpt([], 2) == [[], []]
+    # the batching config's 24 layers over 8 replicas: LPT within 4/3 of the optimum bound
+    ls = gen.batch_layers()
+    cost = [2.0 * c["col"].size * c["N"] for c in ls]
+    per = shard.assign_layers_lpt(cost, 8)
+    loads = [sum(cost[i] for i in r) for r in per]
+    assert max(loads) <= 4.0 / 3.0 * max(sum(cost) / 8, max(cost)) + 1e-9
+
+
+def _rank_cols(rank, world, port, seed):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        rng = np.random.default_rng(seed)
+        N = 40
+        c = gen.small(rng, 131, 77, N, 0.15, empty_rows=0.1)
+        dY = rng.standard_normal((c["M"], N))
+        b = shard.partition_cols(N, world)
+        c0, c1 = int(b[rank]), int(b[rank + 1])
+        Bk = c["B"][:, c0:c1]
+        y_local = torch.from_numpy(oracle.spmm_f64(c["row_ptr"], c["col"], c["vals"], Bk))
+        y = shard.gather_cols(y_local, b).numpy()
+        np.testing.assert_array_equal(y, oracle.spmm_f64(c["row_ptr"], c["col"], c["vals"], c["B"]))
+        # partial dA = SDDMM(dY_k, B_k) on A's pattern, summed over the ranks
+        rows = np.repeat(np.arange(c["M"]), np.diff(c["row_ptr"]))
+        B64 = c["B"].astype(np.float64)
+        part = np.einsum("ij,ij->i", dY[rows][:, c0:c1], B64[c["col"]][:, c0:c1])
+        dA = shard.reduce_grad_a(torch.from_numpy(part)).numpy()
+        full = np.einsum("ij,ij->i", dY[rows], B64[c["col"]])
+        assert np.linalg.norm(dA - full) <= 1e-12 * np.linalg.norm(full)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_gather_cols_and_sum_grad_a():
+    import torch.multiprocessing as mp
+    mp.spawn(_rank_cols, args=(2, _free_port(), 321), nprocs=2, join=True)
