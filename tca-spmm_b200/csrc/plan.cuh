@@ -123,7 +123,7 @@ struct SpmmJob {
     int n_tile; // tensor-core N-slice width (64, 128, 256; 128 or 256 for E4M3)
     // E4M3 forward: B quantized per column (K x N bytes, row stride ldq) with
     // its column scales; A's E4M3 form lives in the plan.
-    int cc_w = 0; // CUDA-core columns per lane (2, 4, 8); 0 = by N
+    int cc_w = 0; // CUDA-core columns per lane (2, 4, 8), 16 = the mma.sync item kernel; 0 = by N
     bool f8 = false;
     const uint8_t *Bq = nullptr;
     int ldq = 0;

@@ -9,11 +9,14 @@
 // so that every B access is a fully used, coalesced 16-byte load with 8 loads
 // in flight per lane.
 //
-// Two kernels:
+// Kernels:
 //   * plan-free (tca_spmm_csr): group g computes caller row g straight from
 //     the CSR, 8 B loads in flight per lane;
-//   * planned (tca_spmm / tca_spmm_batched): groups stream through work items
-//     of consecutive sorted rows of one or many plans (see below).
+//   * planned (tca_spmm / tca_spmm_batched): warps stream through work items
+//     of consecutive sorted rows of one or many plans (spmm_cc_stream_kernel,
+//     below; spmm_cc_items_kernel for operands that are not 16-byte aligned),
+//     or compute them as small mma.sync products (spmm_cc_mma_kernel, an
+//     autotuner candidate for FP16).
 //
 // Malformed CSR never faults: row ranges are clamped to [0, nnz] and
 // nonzeros whose column is outside [0, K) contribute nothing.
