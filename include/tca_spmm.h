@@ -194,7 +194,10 @@ TCA_API int tca_spmm_batched(const tca_batch_item_t *items, int n_items, int c_d
 /* ------------------------------------------------------------------ */
 /* dA on A's pattern (SDDMM): out[j] = alpha * sum_n dY[r_j, n] * B[c_j, n]
  * for every nonzero j in the caller's CSR order; dY is M x N (ldy), B is
- * K x N (ldb), out is nnz values of out_dtype (F16 or F32). */
+ * K x N (ldb), out is nnz values of out_dtype (F16 or F32). Where A is dense
+ * enough (and M * K * 4 <= 256 MiB) it computes dY B^T with one cuBLAS GEMM
+ * into stream-ordered scratch from the library's pool and samples it; else a
+ * sparse kernel; FP32 accumulation either way. */
 TCA_API int tca_sddmm(tca_plan_t plan, const void *d_dY_f16, int ldy, const void *d_B_f16, int ldb, int N,
                       void *d_out, int out_dtype, float alpha, tca_stream_t stream);
 /* dB = alpha * A^T dY + beta * dB (dY M x N, dB K x N of dB_dtype). Runs the
