@@ -21,9 +21,11 @@ L2 and every problem is read from HBM.
              sequential) and the differentiation config (forward vs forward +
              SDDMM + transpose SpMM, gradient errors vs FP64)
 
---impl reference runs the reference's own TCA kernel (our_spmm_balanced,
-built from the reference sources into oracle/_ref) through its host API on
-the same problems, plus the reference's cuSPARSE comparator.
+--impl reference times the reference's own CPU implementation of the
+product, naive_gemm (built from the reference sources into oracle/_ref), on
+the host cores over a bounded sample of the workload per step; the line also
+carries, under reference_gpu, the reference's TCA kernel (our_spmm_balanced)
+through its host API on the same problems and its cuSPARSE comparator.
 
 Multi-GPU (torchrun): each rank runs its own G problems (row-independent
 work, no collective on the data path): weak scaling.
@@ -502,26 +504,52 @@ def run_reference(args, world, rank):
             A = oracle.csr_to_dense(c["M"], c["K"], c["row_ptr"], c["col"], c["vals"])
             _, ms_sp = oracle.ref_cusparse_spmm(A, c["B"], n_iter=n_iter)
             sp_ms.append(ms_sp)
-    value = flops / (sum(ms_kernel) * 1e-3) / 1e9
-    e2e = flops / wall / 1e9
+    gpu_value = flops / (sum(ms_kernel) * 1e-3) / 1e9
+    gpu_e2e = flops / wall / 1e9
     h2d = sum(c["row_ptr"].nbytes + c["col"].nbytes + c["vals"].nbytes + c["B"].nbytes + c["M"] * args.n * 4
               for c in distinct) // len(distinct)
     d2h = distinct[0]["M"] * args.n * 4
+
+    # The arm proper: the reference's own CPU implementation of C = A B,
+    # naive_gemm (src/miscalleneous.cu:114-134: dense FP32-accumulate GEMM,
+    # OpenMP over the rows, all host threads), on a bounded sample per step:
+    # every 16th row of the first problem (the sample keeps the skewed row
+    # lengths), counted by the metric's useful flops 2 nnz(sample) N.
+    c = distinct[0]
+    rows = np.arange(0, c["M"], 16)
+    A_s = oracle.csr_to_dense(c["M"], c["K"], c["row_ptr"], c["col"], c["vals"])[rows]
+    nnz_s = int(np.diff(c["row_ptr"])[rows].sum())
+    cores = len(os.sched_getaffinity(0))
+    for _ in range(max(1, args.warmup)):
+        oracle.ref_naive_gemm(A_s, c["B"])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.ref_naive_gemm(A_s, c["B"])
+    el = time.perf_counter() - t0
+    value = 2.0 * nnz_s * args.n * args.steps / el / 1e9
+    sample = (f"naive_gemm on rows 0, 16, .. of one {c['M']}x{c['K']} problem ({rows.size} rows, "
+              f"nnz {nnz_s}, N={args.n}), {args.steps} steps in {el:.1f} s")
     out = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(sum(ms_kernel) / len(ms_kernel), 5),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el / args.steps * 1e3, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
         "data": "synthetic (seeded numpy PCG64)",
-        "config": {"workload": WORKLOAD, "problems": len(distinct), "N": args.n,
-                   "timing": "the reference's own event timing of n_iter back-to-back launches per call "
-                             "(src/our_spmm.cu:552-574), hot L2; FP32 output"},
-        "reference_impl": "our_spmm_balanced (TCA kernel, mma.sync) from the unmodified reference sources, "
-                          "compiled for sm_100a into oracle/_ref/libtcaref.so; run through its host API",
-        "cpu_baseline": None,
-        "cusparse": {"value": round(flops / (sum(sp_ms) * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
-                     "impl": "perform_cuSPARSE_SpMM (reference comparator, cusparseSpMM CSR ALG_DEFAULT)"},
-        "e2e": {"value": round(e2e, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "path": "our_spmm_balanced(n_iter=1), wall clock"},
+        "config": {"workload": WORKLOAD, "N": args.n, "sample": sample},
+        "reference_impl": "naive_gemm (the reference's CPU implementation of the product) from the unmodified "
+                          "reference sources in oracle/_ref/libtcaref.so, on the host cores",
+        "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": {
+            "value": round(gpu_value, 3), "unit": "GFLOP/s", "problems": len(distinct),
+            "impl": "our_spmm_balanced (TCA kernel, mma.sync) from the unmodified reference sources, compiled "
+                    "for sm_100a into oracle/_ref/libtcaref.so; run through its host API",
+            "timing": "the reference's own event timing of n_iter back-to-back launches per call "
+                      "(src/our_spmm.cu:552-574), hot L2; FP32 output",
+            "e2e": {"value": round(gpu_e2e, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "path": "our_spmm_balanced(n_iter=1), wall clock"},
+            "cusparse": {"value": round(flops / (sum(sp_ms) * 1e-3) / 1e9, 3), "unit": "GFLOP/s",
+                         "impl": "perform_cuSPARSE_SpMM (reference comparator, cusparseSpMM CSR ALG_DEFAULT)"}},
     }
     return out, distinct
 
