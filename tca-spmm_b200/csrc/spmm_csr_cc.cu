@@ -501,10 +501,11 @@ __device__ __forceinline__ void fma_vec(float *acc, unsigned short v, const V &b
 // multiplies the FP32 sum by row scale x column scale, as the tensor-core
 // epilogue does.
 //
-// Three blocks per SM (80 registers a thread): two of them fit beside the
-// tensor-core kernel's block when both paths run concurrently. U B loads are
-// in flight per lane: 8, or 4 at W = 8, which keeps the register budget
-// without spills.
+// Three blocks per SM (80 registers a thread). Beside the tensor-core
+// kernel's block one of them is resident at a time (a warp's registers come
+// from its SM sub-partition, and the tensor-core warps leave room for two
+// more warps per sub-partition). U B loads are in flight per lane: 8, or 4
+// at W = 8, which keeps the register budget without spills.
 template <typename OutT, int W, bool F8>
 __global__ void __launch_bounds__(256, 3) spmm_cc_stream_kernel(const __grid_constant__ CcBatch b)
 {
@@ -997,9 +998,11 @@ __global__ void __launch_bounds__(kMmaWarps * 32, 2) spmm_cc_mma_kernel(const __
 // one block per SM holds that many registers. It is issued as a programmatic
 // dependent of that launch (which triggers at entry), so its blocks start as
 // soon as the tensor-core blocks are resident, and its grid is cut to the
-// blocks that fit beside them (a block that waited for the tensor-core kernel
-// to end would start its fixed share of the items late). The kernel reads
-// nothing the tensor-core kernel writes, so it never waits on it.
+// blocks that the SM's registers as a whole leave beside them (two per SM:
+// the first starts at once, the second when the first ends -- measured
+// faster than both a wider first block and claiming items from a counter
+// with more blocks). The kernel reads nothing the tensor-core kernel writes,
+// so it never waits on it.
 template <typename OutT, int W, bool F8>
 int launch_stream_group(const CcBatch &b, int beside_regs, cudaStream_t s)
 {
