@@ -164,14 +164,14 @@ int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals
         if ((st = dev_malloc((void **)&d_v, 2 * (size_t)(nnz > 0 ? nnz : 1), nullptr)) != TCA_OK) break;
         if ((st = dev_malloc((void **)&d_B, 2 * (size_t)(K > 0 ? K : 1) * N, nullptr)) != TCA_OK) break;
         if ((st = dev_malloc(&d_C, c_elem * (size_t)M * N, nullptr)) != TCA_OK) break;
-        if ((e = cudaMemcpy(d_rp, h_row_ptr, sizeof(int) * (size_t)(M + 1), cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+        if ((e = cudaMemcpyAsync(d_rp, h_row_ptr, sizeof(int) * (size_t)(M + 1), cudaMemcpyHostToDevice, nullptr)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
         if (nnz > 0) {
-            if ((e = cudaMemcpy(d_ci, h_col_idx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
-            if ((e = cudaMemcpy(d_v, h_vals_f16, 2 * (size_t)nnz, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+            if ((e = cudaMemcpyAsync(d_ci, h_col_idx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, nullptr)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+            if ((e = cudaMemcpyAsync(d_v, h_vals_f16, 2 * (size_t)nnz, cudaMemcpyHostToDevice, nullptr)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
         }
-        if (K > 0 && (e = cudaMemcpy(d_B, h_B_f16, 2 * (size_t)K * N, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+        if (K > 0 && (e = cudaMemcpyAsync(d_B, h_B_f16, 2 * (size_t)K * N, cudaMemcpyHostToDevice, nullptr)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
         if (flags & TCA_FLAG_KEEP_EMPTY_ROWS) {
-            if ((e = cudaMemcpy(d_C, h_C, c_elem * (size_t)M * N, cudaMemcpyHostToDevice)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+            if ((e = cudaMemcpyAsync(d_C, h_C, c_elem * (size_t)M * N, cudaMemcpyHostToDevice, nullptr)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
         }
         tca_plan_opts_t opts;
         tca_plan_opts_default(&opts);
@@ -189,6 +189,11 @@ int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals
         if (elapsed_ms) *elapsed_ms = (double)ms / n_iter;
         if ((e = cudaMemcpy(h_C, d_C, c_elem * (size_t)M * N, cudaMemcpyDeviceToHost)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
     } while (0);
+    // the inputs were copied without a wait (one stream orders everything up
+    // to the synchronous copy-back); on an early exit let those copies end
+    // before the caller gets its buffers back
+    if (st != TCA_OK)
+        cudaStreamSynchronize(nullptr);
     if (plan) tca_plan_destroy(plan);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);

@@ -494,6 +494,10 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     k_permute<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(p->perm, row_ptr, col, val, p->p_row_ptr, M,
                                                                  p->p_col, p->p_val, p->src);
     TCA_CUDA_TRY(cudaGetLastError());
+    // the sorted row offsets on the host (for the work items, step 7), read
+    // back with the window statistics under one synchronisation
+    std::vector<int> h_rp((size_t)M + 1);
+    TCA_CUDA_TRY(cudaMemcpyAsync(h_rp.data(), p->p_row_ptr, sizeof(int) * h_rp.size(), cudaMemcpyDeviceToHost, s));
 
     // 3. windows
     const int W = (M + kWindowRows - 1) / kWindowRows;
@@ -520,8 +524,8 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         TCA_CUDA_TRY(cudaMemcpyAsync(h_nnz.data(), d_wn, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
         TCA_CUDA_TRY(cudaMemcpyAsync(h_elig.data(), d_el, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
         TCA_CUDA_TRY(cudaMemcpyAsync(h_nblk.data(), d_nb, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
-        TCA_CUDA_TRY(cudaStreamSynchronize(s));
     }
+    TCA_CUDA_TRY(cudaStreamSynchronize(s));
 
     // 4. path decision (host, deterministic)
     // A window's chunks are "direct" (the 64-column blocks of K it touches,
@@ -628,23 +632,21 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         TCA_CUDA_TRY(cudaGetLastError());
     }
 
-    // 7. CUDA-core work items
-    std::vector<int> h_rp((size_t)M + 1);
-    TCA_CUDA_TRY(cudaMemcpyAsync(h_rp.data(), p->p_row_ptr, sizeof(int) * h_rp.size(), cudaMemcpyDeviceToHost, s));
-    TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    // 7. CUDA-core work items. The host arrays copied to the device here (and
+    // above) may be reused or freed as soon as the copy call returns: a copy
+    // from pageable host memory returns once the data is staged.
     std::vector<int2> items;
     build_items(cc_list, h_rp, M, items);
     p->n_cc_items = (int)items.size();
     TCA_TRY(dev_alloc(&p->cc_items, items.size(), bytes));
     if (!items.empty())
         TCA_CUDA_TRY(cudaMemcpyAsync(p->cc_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
-    TCA_CUDA_TRY(cudaStreamSynchronize(s));
     build_items(h_all, h_rp, M, items);
     p->n_all_items = (int)items.size();
     TCA_TRY(dev_alloc(&p->all_items, items.size(), bytes));
     if (!items.empty())
         TCA_CUDA_TRY(cudaMemcpyAsync(p->all_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
-    TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    TCA_CUDA_TRY(cudaStreamSynchronize(s)); // the plan is complete, for work on any stream
     return TCA_OK;
 }
 
