@@ -91,19 +91,34 @@ TCA_API void perform_GemmEx(half *A, half *B, float *C, int M, int N, int K, int
 TCA_API void smtx_input_to_Dense(std::ifstream &fin, half **mat, char *filename, int *nRow, int *nCol,
                                  int *nnz);
 
-/* src/file_input.cuh:9 declares this (its body, :194-196, is empty): reads an
- * .smtx file straight into a malloc'd CSR (values 1.0 unless a values line is
- * present). `arg` is unused. */
-TCA_API void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, void *arg = NULL);
-
 /* src/general.cuh:54-59 */
 typedef enum entry_dtype { fp16, fp32, fp64 } entry_dtype;
 
-/* src/arg_parse.h:15-31 -- the reference's run options, layout-identical (the
+/* src/arg_parse.h:15-161 -- the reference's run options, layout-identical (the
  * MatrixMarket readers take a pointer to it and read pattern_only and
- * input_is_zero_based). The command-line parsing constructor of the reference
- * is not provided (its CLI is outside this library); the default constructor
- * sets the reference's defaults (src/general.cuh:21-28, src/arg_parse.h:33-48). */
+ * input_is_zero_based). Both constructors start from the reference's defaults
+ * (src/general.cuh:21-28, src/arg_parse.h:33-48: M = N = K = 1024, 10
+ * iterations, sparsity 0.8, tolerance 1e-3, FP16 A/B, FP32 C, zero-based,
+ * Blocked-ELL block 32).
+ *
+ * Arguments(argc, argv) then parses the reference's getopt options
+ * (src/arg_parse.h:54-133), with the same meaning:
+ *   -m M  -n N  -k K  -i num_iter  -t tolerance  -s target_sparsity
+ *   -f input file (must exist; sets input_file_exists)
+ *   -p 1: pattern_only    -b 0: input_is_zero_based, else one-based
+ *   -e ell_block_size     -d 0 (FP16 A/B, FP32 C) or 2 (FP64 A, B, C)
+ * Unknown options are reported by getopt and skipped, as in the reference.
+ * A missing input file, a -d other than 0 or 2, or a malformed number prints
+ * an error and exits with EXIT_FAILURE like the reference (whose std::stoi
+ * throws on a malformed number); after tca_compat_set_exit_on_error(0) it
+ * sets tca_last_error_string() and keeps the default for that option.
+ * Differences: parsing restarts at argv[1] on every call (getopt's optind is
+ * reset, so a second Arguments in one process parses its own argv), and
+ * input_fname is a malloc'd copy with room for its terminator (the
+ * reference's copy is one byte short). As in the reference, the destructor
+ * does not free input_fname. The constructor prints nothing (the reference's
+ * constructor calls print(), whose body is compiled out at its default
+ * VERBOSE = false); print() writes the settings in the reference's layout. */
 class TCA_API Arguments
 {
 public:
@@ -120,6 +135,9 @@ public:
     char *input_fname;
     int ell_block_size;
     Arguments();
+    Arguments(int argc, char *argv[]);
+    void ParseArgs(int argc, char *argv[]);
+    void print();
 };
 
 /* src/file_input.cuh:6-7, src/file_input.cu:8-134 -- MatrixMarket coordinate
@@ -132,8 +150,10 @@ public:
  * reads out of bounds. */
 TCA_API void mtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg);
 TCA_API void mtx_input_to_Dense(std::ifstream &fin, half **mat, Arguments *arg);
-/* src/file_input.cuh:9 with the reference's parameter type. */
-TCA_API void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg);
+/* src/file_input.cuh:9 declares this (its body, src/file_input.cu:194-196,
+ * is empty): reads an .smtx file straight into a malloc'd CSR (values 1.0
+ * unless a values line is present). `arg` is unused; NULL is accepted. */
+TCA_API void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg = NULL);
 
 /* src/general.cuh:135-138, src/miscalleneous.cu:29-112 */
 TCA_API void convert_dense_to_csr(half *mat, CSR **descr, int nRow, int nCol);

@@ -5,6 +5,8 @@
 // format_conversion). Reference citations are file:line in the reference.
 #include <algorithm>
 #include <cerrno>
+#include <climits>
+#include <unistd.h>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -470,9 +472,9 @@ void smtx_input_to_Dense(std::ifstream &fin, half **mat, char *filename, int *nR
     std::free(rp); std::free(ci); std::free(v);
 }
 
-void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, void *arg)
+void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg)
 {
-    (void)arg;
+    (void)arg; // unused, as the reference's declaration (src/file_input.cuh:9)
     std::ostringstream ss;
     ss << fin.rdbuf();
     const std::string s = ss.str();
@@ -612,6 +614,122 @@ Arguments::Arguments()
 {
 }
 
+Arguments::Arguments(int argc, char *argv[]) : Arguments()
+{
+    ParseArgs(argc, argv);
+}
+
+namespace {
+
+// std::stoi / std::stof acceptance (leading blanks, a number, anything after
+// it ignored), without the exception: false when no number starts the text.
+bool opt_int(const char *s, int *out)
+{
+    errno = 0;
+    char *end = nullptr;
+    const long v = std::strtol(s, &end, 10);
+    if (end == s || errno == ERANGE || v < INT_MIN || v > INT_MAX)
+        return false;
+    *out = (int)v;
+    return true;
+}
+
+bool opt_float(const char *s, float *out)
+{
+    errno = 0;
+    char *end = nullptr;
+    const float v = std::strtof(s, &end);
+    if (end == s || errno == ERANGE)
+        return false;
+    *out = v;
+    return true;
+}
+
+// The reference exits on these errors (src/arg_parse.h:113-116, :121-124);
+// with exit-on-error off the error is recorded and parsing goes on.
+void args_fail(const char *fmt, const char *what)
+{
+    tca::set_error(TCA_ERR_INVALID_ARG, fmt, what);
+    compat_fail(TCA_ERR_INVALID_ARG);
+}
+
+} // namespace
+
+// The options of src/arg_parse.h:54-133 ("m:n:k:i:t:s:f:d:p:b:e:").
+void Arguments::ParseArgs(int argc, char *argv[])
+{
+    optind = 1; // every call parses its own argv from the start
+    int c;
+    while ((c = getopt(argc, argv, "m:n:k:i:t:s:f:d:p:b:e:")) != -1) {
+        int iv = 0;
+        float fv = 0.f;
+        switch (c) {
+        case 'm': case 'n': case 'k': case 'i': case 'e': case 'p': case 'b': case 'd':
+            if (!opt_int(optarg, &iv)) {
+                args_fail("option value '%s' is not an integer", optarg);
+                break;
+            }
+            if (c == 'm') M = iv;
+            else if (c == 'n') N = iv;
+            else if (c == 'k') K = iv;
+            else if (c == 'i') num_iter = iv;
+            else if (c == 'e') ell_block_size = iv;
+            else if (c == 'p') pattern_only = iv == 1;
+            else if (c == 'b') input_is_zero_based = iv == 0;
+            else if (iv == (int)fp16) { a_type = b_type = fp16; c_type = fp32; }
+            else if (iv == (int)fp64) { a_type = b_type = c_type = fp64; }
+            else args_fail("Not Implemented error for the specified dtype (-d %s)", optarg);
+            break;
+        case 't': case 's':
+            if (!opt_float(optarg, &fv)) {
+                args_fail("option value '%s' is not a number", optarg);
+                break;
+            }
+            if (c == 't') tolerance = fv;
+            else target_sparsity = fv;
+            break;
+        case 'f': {
+            const size_t n = std::strlen(optarg);
+            input_fname = (char *)std::malloc(n + 1);
+            std::memcpy(input_fname, optarg, n + 1);
+            break;
+        }
+        default: // getopt reported the unknown option; skipped as in the reference
+            break;
+        }
+    }
+    input_file_exists = false;
+    if (input_fname != nullptr) {
+        if (access(input_fname, F_OK) != 0)
+            args_fail("Input file not exists error: %s", input_fname);
+        else
+            input_file_exists = true;
+    }
+}
+
+// src/arg_parse.h:135-160 (the reference's layout of the same settings).
+void Arguments::print()
+{
+    static const char *dt[] = {"FP16", "FP32", "FP64"};
+    std::printf("===================== Arguments ==========================\n");
+    std::printf("Tolerance : %f\n", tolerance);
+    std::printf("A type : %s, B type : %s, C type : %s\n", dt[a_type], dt[b_type], dt[c_type]);
+    std::printf("N iter : %d\n", num_iter);
+    std::printf("Ell block size : %d \n", ell_block_size);
+    if (input_fname == nullptr) {
+        std::printf("No input file have been passed ... generate synthetic with random entries\n");
+        std::printf("The matrix size .. M: %d , N: %d, K: %d\n", M, N, K);
+        std::printf("Target Sparsity : %f\n", target_sparsity);
+    } else {
+        std::printf("Input file name : %s\n", input_fname);
+    }
+    if (pattern_only)
+        std::printf("Matrix is specified as pattern only matrix\n");
+    if (!input_is_zero_based)
+        std::printf("Input matrix is specified as one based index matrix\n");
+    std::printf("================== End of Arguments ======================\n");
+}
+
 static std::string slurp(std::ifstream &fin)
 {
     std::ostringstream ss;
@@ -645,9 +763,4 @@ void mtx_input_to_Dense(std::ifstream &fin, half **mat, Arguments *arg)
     *mat = (half *)std::malloc(sizeof(half) * (size_t)M * K + 1);
     tca_csr_to_dense(M, K, nnz, rp, ci, v, *mat);
     std::free(rp); std::free(ci); std::free(v);
-}
-
-void smtx_input_to_CSR(std::ifstream &fin, CSR **csr_mat, Arguments *arg)
-{
-    smtx_input_to_CSR(fin, csr_mat, static_cast<void *>(arg));
 }

@@ -1,3 +1,4 @@
+import os
 import pathlib
 import sys
 
@@ -8,7 +9,10 @@ for p in (ROOT, ROOT / "tca-spmm_b200" / "python"):
     if str(p) not in sys.path:
         sys.path.insert(0, str(p))
 
-REFERENCE_TREE = pathlib.Path("/root/reference")
+# The reference project's tree (only for the tests that read its files; they
+# skip when it is not given): the environment variable TCA_REFERENCE_ROOT.
+_ref_env = os.environ.get("TCA_REFERENCE_ROOT")
+REFERENCE_TREE = pathlib.Path(_ref_env) if _ref_env else None
 
 
 def pytest_configure(config):

@@ -16,14 +16,28 @@ oracle/_ref/libtcaref.so (`make -C oracle ref`):
   mtx_*.mtx              seeded MatrixMarket files (written by this script)
     mtx_<i>_csr_*        mtx_input_to_CSR (src/file_input.cu:63-134) on mtx_<i>.mtx
     mtx_<i>_dense        mtx_input_to_Dense (src/file_input.cu:8-62) on mtx_<i>.mtx
+  body_decoder_layer_2_ffn_conv1.smtx
+                         the reference's only data fixture (data/ in the
+                         reference project), copied unchanged
+    fixture_shape, fixture_coords
+                         smtx_input_to_Dense on it, stored as for smtx_<i>
+    args_<i>             the fields of the reference's Arguments(argc, argv)
+                         (src/arg_parse.h:33-133) for the argv ARGS_CASES[i],
+                         printed by a small driver compiled against the
+                         reference's own header
 
-Run from the repository root:  python tests/golden/make_golden.py
+The reference project is located by the environment variable
+TCA_REFERENCE_ROOT. Run from the repository root:
+    TCA_REFERENCE_ROOT=<reference project> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
+import os
 import pathlib
+import shutil
 import subprocess
 import sys
+import tempfile
 
 import numpy as np
 
@@ -105,8 +119,56 @@ MTX_CASES = [  # (M, K, n, one_based, with_values, missing_every, pattern_only)
 ]
 
 
+# argv of Arguments(argc, argv) cases (argv[0] is the program name). Option
+# -f, whose copy the reference makes one byte short of its terminator, is
+# checked against known answers in the tests instead.
+ARGS_CASES = [
+    [],
+    ["-m", "2048", "-n", "256", "-k", "512", "-i", "20", "-t", "0.01", "-s", "0.95", "-p", "1", "-b", "1",
+     "-e", "16", "-d", "2"],
+    ["-d", "0", "-p", "0", "-b", "0", "-s", "1e-1", "-t", "2.5e-4"],
+    ["-m", "12abc", "-n", " 64", "-q", "-k", "-7"],
+]
+
+# Prints the fields of Arguments(argc, argv); compiled against the
+# reference's src/arg_parse.h (USE_REFERENCE) or this project's
+# include/tca_spmm_compat.h (the tests).
+ARGS_DRIVER = r'''
+#ifdef USE_REFERENCE
+#include "arg_parse.h"
+#else
+#include "tca_spmm_compat.h"
+#endif
+#include <cstdio>
+int main(int argc, char **argv)
+{
+    Arguments a(argc, argv);
+    std::printf("%d %d %d %d %d %d %d %a %a %d %d %d %d\n", a.M, a.N, a.K, a.num_iter, (int)a.pattern_only,
+                (int)a.input_is_zero_based, (int)a.input_file_exists, (double)a.target_sparsity,
+                (double)a.tolerance, (int)a.a_type, (int)a.b_type, (int)a.c_type, a.ell_block_size);
+    return 0;
+}
+'''
+
+
+def reference_args(ref_src):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    with tempfile.TemporaryDirectory() as d:
+        src = pathlib.Path(d) / "args_ref.cu"
+        src.write_text(ARGS_DRIVER)
+        exe = pathlib.Path(d) / "args_ref"
+        subprocess.run([nvcc, "-std=c++17", "-DUSE_REFERENCE", "-I", str(ROOT / "oracle" / "stub"), "-I",
+                        str(ref_src), str(src), "-o", str(exe)], check=True)
+        return [subprocess.run([str(exe)] + argv, capture_output=True, text=True, check=True).stdout.strip()
+                for argv in ARGS_CASES]
+
+
 def main():
-    subprocess.run(["make", "-C", str(ROOT / "oracle"), "all", "ref"], check=True)
+    ref_root = os.environ.get("TCA_REFERENCE_ROOT")
+    if not ref_root:
+        sys.exit("set TCA_REFERENCE_ROOT to the reference project's directory")
+    ref_root = pathlib.Path(ref_root)
+    subprocess.run(["make", "-C", str(ROOT / "oracle"), "all", "ref", f"REF_SRC={ref_root / 'src'}"], check=True)
     rng = np.random.default_rng(20240601)
     g = {}
     for i, (M, K, row_ptr, col) in enumerate(smtx_cases(rng)):
@@ -139,6 +201,14 @@ def main():
         g[f"mtx_{i}_csr_shape"] = np.array([m, k], np.int64)
         g[f"mtx_{i}_csr_row_ptr"], g[f"mtx_{i}_csr_col"], g[f"mtx_{i}_csr_val"] = rp, ci, v
         g[f"mtx_{i}_dense"] = D
+    fixture = next((ref_root / "data").glob("*.smtx"))
+    shutil.copyfile(fixture, OUT / fixture.name)
+    A, nnz = oracle.ref_smtx_to_dense(OUT / fixture.name)
+    r, c = np.nonzero(A.view(np.uint16))
+    g["fixture_shape"] = np.array([A.shape[0], A.shape[1], nnz], np.int64)
+    g["fixture_coords"] = np.stack([r, c]).astype(np.int32)
+    for i, line in enumerate(reference_args(ref_root / "src")):
+        g[f"args_{i}"] = np.array(line)
     np.savez_compressed(OUT / "golden.npz", **g)
     print("wrote", OUT / "golden.npz", len(g), "arrays")
 

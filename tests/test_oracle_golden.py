@@ -85,7 +85,21 @@ def test_reference_warp_demand_bins():
     assert list(d) == [0, 1, 1, 2, 2, 4, 4, 8, 8, 8 * 2, 8 * 4, 8 * 4]
 
 
-@pytest.mark.skipif(not (REFERENCE_TREE / "data").exists(), reason="reference tree not mounted")
+def test_reference_fixture_parse(golden):
+    """The reference's own data file (copied into tests/golden/ by
+    make_golden.py), parsed by the oracle, against the reference's
+    smtx_input_to_Dense output recorded beside it."""
+    path = ROOT / "tests" / "golden" / "body_decoder_layer_2_ffn_conv1.smtx"
+    M, K, nnz, rp, ci = oracle.smtx_parse(path.read_bytes())
+    assert (M, K, nnz) == tuple(golden["fixture_shape"])
+    r, c = golden["fixture_coords"]
+    assert np.array_equal(np.repeat(np.arange(M), np.diff(rp)), r)
+    assert np.array_equal(ci, c)
+    assert (np.diff(rp) > 64).any()  # exercises the reference's long-row path
+
+
+@pytest.mark.skipif(REFERENCE_TREE is None or not (REFERENCE_TREE / "data").exists(),
+                    reason="TCA_REFERENCE_ROOT not set")
 def test_reference_fixture_parse_live():
     """The reference's own data file, parsed by the oracle and by the
     reference's smtx_input_to_Dense (oracle/_ref), must agree exactly."""
