@@ -21,11 +21,19 @@ L2 and every problem is read from HBM.
              sequential) and the differentiation config (forward vs forward +
              SDDMM + transpose SpMM, gradient errors vs FP64)
 
+  per_problem  one problem per call at every point of the forward target
+             (4096 x 1024 at 70-98 % sparsity, N = 64-512): this project, the
+             reference's TCA kernel with its own schedule and the reference
+             comparator's cuSPARSE call on the same device buffers, timed the
+             same way (CUDA graph of 100 calls hot; one call after an L2 flush
+             cold), with speed-ups, roofline fractions and errors vs FP64
+
 --impl reference times the reference's own CPU implementation of the
 product, naive_gemm (built from the reference sources into oracle/_ref), on
-the host cores over a bounded sample of the workload per step; the line also
-carries, under reference_gpu, the reference's TCA kernel (our_spmm_balanced)
-through its host API on the same problems and its cuSPARSE comparator.
+the host cores: the whole first problem per step when the run fits in
+REF_BUDGET_S, else a row sample; the line also carries, under reference_gpu,
+the reference's TCA kernel (our_spmm_balanced) through its host API on the
+same problems and its cuSPARSE comparator.
 
 Multi-GPU (torchrun): each rank runs its own G problems (row-independent
 work, no collective on the data path): weak scaling.
@@ -48,6 +56,7 @@ sys.path.insert(0, str(ROOT / "tca-spmm_b200" / "python"))
 sys.path.insert(0, str(ROOT))
 
 METRIC = "SpMM GFLOP/s (2*nnz*N), FP16 in, FP32 accumulate, FP16 out"
+REF_BUDGET_S = 120.0  # CPU seconds the reference arm's warm-up + timed steps may take
 WORKLOAD = "sweep 4096x1024 sparsity 0.80 zipf(1.2) N=256"
 
 
@@ -62,6 +71,7 @@ def parse():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-per-problem", action="store_true", help="skip the per-problem comparison leg")
     return ap.parse_args()
 
 
@@ -354,6 +364,7 @@ def run_ours(args, world, rank):
         "fp8": fp8,
         "batching": batching_leg(args, world),
         "fwd_bwd": fwd_bwd_leg(args, rank == 0 and not args.no_cpu),
+        "per_problem": per_problem_leg(args, rank == 0 and not args.no_cpu) if not args.no_per_problem else None,
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
     }
@@ -423,6 +434,139 @@ def batching_leg(args, world):
             "graph_us": round(t_graph, 2), "sequential_us": round(t_seq, 2),
             "speedup": round(t_seq / t_graph, 3), "graph_gflops": round(flops / (t_graph * 1e-6) / 1e9, 1),
             "tuned": [list(t) for t in tuned]}
+
+
+# (sparsity, N) of the per-problem comparison: the sweep matrix 4096 x 1024
+# (Zipf(1.2) rows) across the sparsities and widths the forward target names
+PER_PROBLEM = [(0.70, 256), (0.80, 256), (0.90, 256), (0.95, 256), (0.98, 256), (0.80, 64), (0.80, 128),
+               (0.80, 512)]
+
+
+def time_hot_cold(torch, fn, flush, n_graph=100, reps=10, cold_reps=20):
+    """Per-call device time of fn (one forward issued on torch's current
+    stream), the same way for every implementation: hot = a CUDA graph of
+    n_graph back-to-back calls, median over reps replays, divided by n_graph;
+    cold = a graph of one call replayed after writing a buffer larger than L2,
+    median over cold_reps replays. Falls back to the same loops without a graph
+    when fn cannot be captured."""
+    s = torch.cuda.Stream()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            fn()
+    torch.cuda.synchronize()
+    method = "cuda graph"
+    try:
+        g, g1 = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+            for _ in range(n_graph):
+                fn()
+        with torch.cuda.graph(g1, stream=s, capture_error_mode="relaxed"):
+            fn()
+        run_n, run_1 = g.replay, g1.replay
+    except Exception:  # noqa: BLE001 -- not capturable: time the plain launches
+        torch.cuda.synchronize()
+        method = "stream loop (not capturable)"
+
+        def run_n():
+            for _ in range(n_graph):
+                fn()
+        run_1 = fn
+    hot, cold = [], []
+    with torch.cuda.stream(s):
+        run_n()
+        for _ in range(reps):
+            a, b = ev(), ev()
+            a.record()
+            run_n()
+            b.record()
+            b.synchronize()
+            hot.append(a.elapsed_time(b) * 1e3 / n_graph)
+        for _ in range(cold_reps):
+            flush.zero_()
+            a, b = ev(), ev()
+            a.record()
+            run_1()
+            b.record()
+            b.synchronize()
+            cold.append(a.elapsed_time(b) * 1e3)
+    torch.cuda.synchronize()
+    return float(np.median(hot)), float(np.median(cold)), method
+
+
+def per_problem_leg(args, check):
+    """One problem per call, at every point of the forward target: this
+    project's forward (FP16 C, the configuration's output, and FP32 C, the
+    comparators' output), the reference's TCA kernel with its own schedule and
+    the reference comparator's cuSPARSE call, all on the same device buffers
+    in this process and timed the same way (time_hot_cold). With `check`,
+    every output's relative Frobenius error against the FP64 oracle."""
+    import torch
+    import tca_spmm
+    from tca_spmm import gen
+    from oracle import oracle
+    dev = torch.device("cuda", torch.cuda.current_device())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # 256 MB > 126 MB L2
+    have_ref = oracle.ref_available()
+    peak, _ = peaks()
+    rows = []
+    for sp, N in PER_PROBLEM:
+        c = gen.sweep(sp, N=N, seed=7000)
+        M, K, nnz = c["M"], c["K"], int(c["col"].size)
+        rp, ci, v, B = (torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+                        for x in (c["row_ptr"], c["col"], c["vals"], c["B"]))
+        plan = tca_spmm.Plan(rp, ci, v, K)
+        outs = {"ours_f16": torch.empty((M, N), dtype=torch.float16, device=dev),
+                "ours_f32": torch.empty((M, N), dtype=torch.float32, device=dev),
+                "reference_tca": torch.zeros((M, N), dtype=torch.float32, device=dev),
+                "cusparse": torch.zeros((M, N), dtype=torch.float32, device=dev)}
+        fns = {"ours_f16": lambda: plan.spmm(B, out=outs["ours_f16"]),
+               "ours_f32": lambda: plan.spmm(B, out=outs["ours_f32"])}
+        closers = []
+        if have_ref:
+            tk = oracle.RefTcaKernel(M, N, K, c["row_ptr"], v.data_ptr(), rp.data_ptr(), ci.data_ptr(),
+                                     B.data_ptr(), outs["reference_tca"].data_ptr())
+            cs = oracle.RefCusparse(M, N, K, nnz, rp.data_ptr(), ci.data_ptr(), v.data_ptr(), B.data_ptr(),
+                                    outs["cusparse"].data_ptr())
+            closers += [tk, cs]
+            fns["reference_tca"] = lambda: tk.launch(torch.cuda.current_stream().cuda_stream)
+            fns["cusparse"] = lambda: cs.launch(torch.cuda.current_stream().cuda_stream)
+        flops = 2.0 * nnz * N
+        bytes16 = nnz * 6 + (M + 1) * 4 + K * N * 2 + M * N * 2
+        row = {"sparsity": sp, "N": N, "nnz": nnz, "us": {}, "cold_us": {}, "timing": {}}
+        for name, fn in fns.items():
+            hot, cold, method = time_hot_cold(torch, fn, flush)
+            row["us"][name], row["cold_us"][name], row["timing"][name] = round(hot, 3), round(cold, 3), method
+        t = row["us"]["ours_f16"]
+        row["gflops_ours_f16"] = round(flops / (t * 1e-6) / 1e9, 1)
+        row["roofline_frac_ours_f16"] = round(bytes16 / (t * 1e-6) / 1e9 / peak, 4)
+        row["roofline_frac_ours_f16_cold"] = round(bytes16 / (row["cold_us"]["ours_f16"] * 1e-6) / 1e9 / peak, 4)
+        if have_ref:
+            for ref_name in ("reference_tca", "cusparse"):
+                row[f"speedup_vs_{ref_name}"] = round(row["us"][ref_name] / t, 3)
+                row[f"speedup_vs_{ref_name}_cold"] = round(row["cold_us"][ref_name] / row["cold_us"]["ours_f16"], 3)
+                row[f"speedup_f32_vs_{ref_name}"] = round(row["us"][ref_name] / row["us"]["ours_f32"], 3)
+        if check:
+            torch.cuda.synchronize()
+            ref = oracle.spmm_f64(c["row_ptr"], c["col"], c["vals"], c["B"])
+            nrm = np.linalg.norm(ref)
+            row["rel_err_vs_f64"] = {k: float(f"{np.linalg.norm(o.double().cpu().numpy() - ref) / nrm:.3e}")
+                                     for k, o in outs.items() if k in fns}
+        for x in closers:
+            x.close()
+        plan.close()
+        rows.append(row)
+    return {"workload": "one 4096x1024 Zipf(1.2) problem per call (seed 7000), B U(-1,1)",
+            "method": "per-call device time: hot = CUDA graph of 100 back-to-back calls (median of 10 replays "
+                      "/ 100); cold = one call per replay after a 256 MB write (median of 20); the same "
+                      "for every implementation, on the same device buffers",
+            "impls": {"ours_f16": "tca_spmm, FP16 C", "ours_f32": "tca_spmm, FP32 C",
+                      "reference_tca": "kernel_our_spmm_balanced<64> with workload_manager's schedule "
+                                       "(reference sources, sm_100a), FP32 C",
+                      "cusparse": "cusparseSpMM CSR ALG_DEFAULT with the reference comparator's parameters, "
+                                  "FP32 C"},
+            "target": "ours_f16 >= 1.5x both reference_tca and cusparse at >= 0.60 of the HBM roofline",
+            "rows": rows}
 
 
 def fwd_bwd_leg(args, check):
@@ -512,14 +656,22 @@ def run_reference(args, world, rank):
 
     # The arm proper: the reference's own CPU implementation of C = A B,
     # naive_gemm (src/miscalleneous.cu:114-134: dense FP32-accumulate GEMM,
-    # OpenMP over the rows, all host threads), on a bounded sample per step:
-    # every 16th row of the first problem (the sample keeps the skewed row
-    # lengths), counted by the metric's useful flops 2 nnz(sample) N.
+    # OpenMP over the rows, all host threads), on the first problem of the
+    # workload, counted by the metric's useful flops 2 nnz N. A step is the
+    # whole problem when warm-up + steps fit in REF_BUDGET_S seconds; else
+    # every r-th row (the sample keeps the skewed row lengths), r as small as
+    # the budget allows.
     c = distinct[0]
-    rows = np.arange(0, c["M"], 16)
-    A_s = oracle.csr_to_dense(c["M"], c["K"], c["row_ptr"], c["col"], c["vals"])[rows]
-    nnz_s = int(np.diff(c["row_ptr"])[rows].sum())
+    A_full = oracle.csr_to_dense(c["M"], c["K"], c["row_ptr"], c["col"], c["vals"])
     cores = len(os.sched_getaffinity(0))
+    oracle.ref_naive_gemm(A_full, c["B"])  # warm-up (thread pool, pages)
+    t0 = time.perf_counter()
+    oracle.ref_naive_gemm(A_full, c["B"])
+    t_full = time.perf_counter() - t0
+    stride = max(1, int(np.ceil((args.steps + args.warmup) * t_full / REF_BUDGET_S)))
+    rows = np.arange(0, c["M"], stride)
+    A_s = A_full[rows] if stride > 1 else A_full
+    nnz_s = int(np.diff(c["row_ptr"])[rows].sum())
     for _ in range(max(1, args.warmup)):
         oracle.ref_naive_gemm(A_s, c["B"])
     t0 = time.perf_counter()
@@ -527,14 +679,19 @@ def run_reference(args, world, rank):
         oracle.ref_naive_gemm(A_s, c["B"])
     el = time.perf_counter() - t0
     value = 2.0 * nnz_s * args.n * args.steps / el / 1e9
-    sample = (f"naive_gemm on rows 0, 16, .. of one {c['M']}x{c['K']} problem ({rows.size} rows, "
-              f"nnz {nnz_s}, N={args.n}), {args.steps} steps in {el:.1f} s")
+    if stride == 1:
+        sample = (f"naive_gemm on the whole {c['M']}x{c['K']} problem (nnz {nnz_s}, N={args.n}) per step, "
+                  f"{args.steps} steps in {el:.1f} s")
+    else:
+        sample = (f"naive_gemm on rows 0, {stride}, .. of one {c['M']}x{c['K']} problem ({rows.size} rows, "
+                  f"nnz {nnz_s}, N={args.n}) per step, {args.steps} steps in {el:.1f} s (the whole problem "
+                  f"takes {t_full:.2f} s: {args.steps + args.warmup} of them exceed {REF_BUDGET_S:.0f} s)")
     out = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el / args.steps * 1e3, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
         "data": "synthetic (seeded numpy PCG64)",
-        "config": {"workload": WORKLOAD, "N": args.n, "sample": sample},
+        "config": {"workload": WORKLOAD, "N": args.n, "sample": sample, "same_config": stride == 1},
         "reference_impl": "naive_gemm (the reference's CPU implementation of the product) from the unmodified "
                           "reference sources in oracle/_ref/libtcaref.so, on the host cores",
         "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": cores, "kind": "reference",

@@ -52,6 +52,13 @@ typedef enum tca_dtype {
  * flag those rows become beta * C. */
 #define TCA_FLAG_KEEP_EMPTY_ROWS 1u
 
+/* Test hook for the device-side failure path, not for production use: in the
+ * tensor-core kernel each CTA withholds the completion signal of its last
+ * accumulator, so that the epilogue's bounded wait for it (about one second)
+ * runs out. The launch then ends normally with those output rows unwritten,
+ * and tca_plan_status reports TCA_ERR_TIMEOUT. */
+#define TCA_FLAG_TEST_WITHHOLD_ACCUM (1u << 31)
+
 /* ------------------------------------------------------------------ */
 /* Library information and errors                                     */
 /* ------------------------------------------------------------------ */
@@ -145,8 +152,10 @@ TCA_API int tca_plan_info(tca_plan_t plan, tca_plan_info_t *info);
  * size. With h_dst NULL only the size is returned. Used to check the GPU build
  * of the format bit for bit against a host build. */
 TCA_API int tca_plan_export(tca_plan_t plan, int which, void *h_dst, size_t capacity_bytes, size_t *out_bytes);
-/* Reads the plan's device status word (synchronises): TCA_ERR_TIMEOUT when a
- * bounded device-side wait of an earlier launch gave up, else TCA_OK. */
+/* Reads and clears the plan's device status word (synchronises):
+ * TCA_ERR_TIMEOUT when a bounded device-side wait of a launch since the last
+ * call gave up, else TCA_OK. The kernel that gave up ends normally (tensor
+ * memory released, no copy left in flight), so the context stays usable. */
 TCA_API int tca_plan_status(tca_plan_t plan);
 TCA_API int tca_plan_destroy(tca_plan_t plan);
 
@@ -250,13 +259,24 @@ TCA_API int tca_spmm_fp8_batched(const tca_batch_item_t *items, int n_items, int
  * TCA_ERR_INVALID_ARG (use tca_spmm_fp8). The plan's E4M3 form must exist
  * already (tca_plan_quantize_fp8, which allocates, called once at set-up).
  * The first call on each device looks up the array's device address; make
- * that first call before any stream capture. Every call on a device shares
- * the one array (the call clears what it needs cleared): calls whose work
- * overlaps on the GPU -- on different streams, or from different threads --
- * race and give wrong results. Otherwise as tca_spmm_fp8. */
+ * that first call before any stream capture. The address is kept for the
+ * process: after a cudaDeviceReset of a device, do not call this on that
+ * device again. Every call on a device shares the one array (the call clears
+ * what it needs cleared): calls whose work overlaps on the GPU -- on
+ * different streams, or from different threads -- race and give wrong
+ * results. K == 0 writes C = beta * C through tca_spmm (no quantization, no
+ * allocation). Otherwise as tca_spmm_fp8, with the same launches. */
 #define TCA_FP8_STATIC_SCRATCH_BYTES (16u << 20)
 TCA_API int tca_spmm_fp8_static(tca_plan_t plan, const void *d_B_f16, int ldb, int N, void *d_C, int ldc, int c_dtype,
                                 float alpha, float beta, unsigned flags, tca_stream_t stream);
+
+/* Device memory the library holds on the current device: its stream-ordered
+ * pool (plans, their temporaries and workspaces, host-buffer calls), in
+ * bytes reserved from the device, in use now, and the highest use since the
+ * last reset (reset_high != 0 resets that mark to the current use first).
+ * Any pointer may be NULL. Diagnostics; no counterpart in the reference,
+ * which allocates with cudaMalloc per call (src/our_spmm.cu:497-506). */
+TCA_API int tca_pool_stats(int reset_high, size_t *reserved_bytes, size_t *used_bytes, size_t *used_high_bytes);
 
 /* ---- Batched forward as a CUDA graph, and its autotuner (no counterpart in
  * the reference: its launch geometry is fixed per call by workload_manager,

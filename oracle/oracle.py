@@ -312,6 +312,12 @@ def ref() -> ctypes.CDLL:
         R.ref_cusparse_blockspmm.restype = None
         R.ref_gemmex.argtypes = [_P, _P, _P, _I, _I, _I, _I, D]; R.ref_gemmex.restype = None
         R.ref_cusparselt_24.argtypes = [_P, _P, _P, _I, _I, _I, _I, D]; R.ref_cusparselt_24.restype = None
+        R.ref_tca_schedule.argtypes = [_I, _I, _I, _I, _P]; R.ref_tca_schedule.restype = _P
+        R.ref_tca_launch.argtypes = [_P, _P, _P, _P, _P, _P, _P]; R.ref_tca_launch.restype = _I
+        R.ref_tca_free.argtypes = [_P]; R.ref_tca_free.restype = None
+        R.ref_cusparse_setup.argtypes = [_I, _I, _I, _I, _P, _P, _P, _P, _P]; R.ref_cusparse_setup.restype = _P
+        R.ref_cusparse_run.argtypes = [_P, _P]; R.ref_cusparse_run.restype = _I
+        R.ref_cusparse_free.argtypes = [_P]; R.ref_cusparse_free.restype = None
         _ref = R
     return _ref
 
@@ -456,6 +462,52 @@ def ref_gemmex(A, B, C=None, n_iter=1):
     ms = ctypes.c_double(-1.0)
     ref().ref_gemmex(Ab.ctypes.data, Bb.ctypes.data, out.ctypes.data, M, N, K, n_iter, ctypes.byref(ms))
     return out, ms.value
+
+
+class RefTcaKernel:
+    """The reference TCA kernel (kernel_our_spmm_balanced<64>) on device
+    buffers with the schedule its own host code builds (workload_manager):
+    launch() issues one forward on the given CUDA stream, C (FP32) = A B.
+    Device pointers are plain integers (e.g. torch's data_ptr())."""
+
+    def __init__(self, M, N, K, row_ptr_host, d_val, d_row_ptr, d_col, d_B, d_C):
+        rp = _c(row_ptr_host, np.int32)
+        self._R = ref()
+        with quiet_stdout():
+            self._h = self._R.ref_tca_schedule(M, N, K, int(rp[-1]), rp.ctypes.data)
+        self._args = (d_val, d_row_ptr, d_col, d_B, d_C)
+
+    def launch(self, stream):
+        rc = self._R.ref_tca_launch(self._h, *self._args, stream)
+        if rc != 0:
+            raise RuntimeError(f"reference kernel launch failed: CUDA error {rc}")
+
+    def close(self):
+        if self._h:
+            self._R.ref_tca_free(self._h)
+            self._h = None
+
+
+class RefCusparse:
+    """The reference comparator's cusparseSpMM call (CSR 32I, FP16 A/B, FP32
+    C and compute, ALG_DEFAULT) on device buffers: launch() issues one
+    forward on the given CUDA stream."""
+
+    def __init__(self, M, N, K, nnz, d_row_ptr, d_col, d_val, d_B, d_C):
+        self._R = ref()
+        self._h = self._R.ref_cusparse_setup(M, N, K, nnz, d_row_ptr, d_col, d_val, d_B, d_C)
+        if not self._h:
+            raise RuntimeError("cuSPARSE set-up failed")
+
+    def launch(self, stream):
+        rc = self._R.ref_cusparse_run(self._h, stream)
+        if rc != 0:
+            raise RuntimeError(f"cusparseSpMM failed: status {rc}")
+
+    def close(self):
+        if self._h:
+            self._R.ref_cusparse_free(self._h)
+            self._h = None
 
 
 class quiet_stdout:

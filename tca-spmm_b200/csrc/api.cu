@@ -128,6 +128,31 @@ int tca_spmm_csr(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_
                               (cudaStream_t)stream);
 }
 
+int tca_pool_stats(int reset_high, size_t *reserved_bytes, size_t *used_bytes, size_t *used_high_bytes)
+{
+    clear_error();
+    cudaMemPool_t pool;
+    TCA_TRY(pool_of_current_device(&pool));
+    if (reset_high) {
+        uint64_t zero = 0; // resets the high mark to the current use
+        TCA_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+    }
+    uint64_t v = 0;
+    if (reserved_bytes) {
+        TCA_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v));
+        *reserved_bytes = (size_t)v;
+    }
+    if (used_bytes) {
+        TCA_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &v));
+        *used_bytes = (size_t)v;
+    }
+    if (used_high_bytes) {
+        TCA_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &v));
+        *used_high_bytes = (size_t)v;
+    }
+    return TCA_OK;
+}
+
 // Host-buffer forward: the reference's calling convention (our_spmm_balanced,
 // src/our_spmm.cu:472-588) -- device buffers are allocated and freed per call,
 // C is uploaded only when it is read (beta-free reference semantics read it for

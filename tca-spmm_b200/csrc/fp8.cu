@@ -493,7 +493,10 @@ std::mutex g_scratch_mutex;
 // Device address of the scratch on the current device. The array's name in
 // host code is only a host-side handle of the symbol; the address a kernel
 // can use comes from cudaGetSymbolAddress, asked once per device with that
-// device current (the first call on each device).
+// device current (the first call on each device). The cached address belongs
+// to the device's primary context: after cudaDeviceReset the module is loaded
+// anew and the cache is stale, so a process that resets a device must not
+// call this entry point on it again.
 int static_scratch(void **out)
 {
     int dev = 0;
@@ -527,8 +530,8 @@ int tca_spmm_fp8_static(tca_plan_t p, const void *d_B_f16, int ldb, int N, void 
     if (N % 8 != 0 || !aligned16(d_C) || ((size_t)ldc * c_elem) % 16 != 0)
         return set_error(TCA_ERR_UNSUPPORTED,
                          "the E4M3 forward needs N %% 8 == 0 and a 16-byte aligned C with 16-byte aligned rows");
-    if (p->K == 0)
-        return set_error(TCA_ERR_UNSUPPORTED, "K == 0: use tca_spmm (nothing to quantize)");
+    if (p->K == 0) // no nonzeros can exist: A B = 0, so C = beta * C, which tca_spmm writes without allocating
+        return tca_spmm(p, d_B_f16, ldb, N, d_C, ldc, c_dtype, alpha, beta, flags, stream);
     if (!p->has_fp8)
         return set_error(TCA_ERR_INVALID_ARG,
                          "the plan has no E4M3 form: call tca_plan_quantize_fp8 once first (it allocates)");
@@ -559,7 +562,7 @@ int tca_spmm_fp8_static(tca_plan_t p, const void *d_B_f16, int ldb, int N, void 
     job.Bq = Bq;
     job.ldq = ldq;
     job.col_scale = scale;
-    // launched directly (no deferred launch list): nothing on this path allocates
-    TCA_TRY(launch_tc_jobs(&job, 1, c_dtype, alpha, beta, flags, s));
-    return launch_cc_jobs(&job, 1, c_dtype, alpha, beta, flags, s);
+    // the same launches as tca_spmm_fp8 (the CUDA-core launch runs beside the
+    // tensor-core launch as its programmatic dependent); they allocate nothing
+    return run_jobs_with_events(&job, 1, c_dtype, alpha, beta, flags, s, nullptr);
 }

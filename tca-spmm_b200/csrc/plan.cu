@@ -812,6 +812,8 @@ int tca_plan_status(tca_plan_t p)
     if (!p->d_status) return TCA_OK;
     int h = 0;
     TCA_CUDA_TRY(cudaMemcpy(&h, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h != 0)
+        TCA_CUDA_TRY(cudaMemset(p->d_status, 0, sizeof(int))); // read and clear
     if (h & kStatusTimeout)
         return set_error(TCA_ERR_TIMEOUT, "a bounded device-side wait gave up (status word 0x%x)", h);
     if (h & kStatusLayout)

@@ -156,8 +156,8 @@ template <int NT, bool F8> struct TcCfg {
     static constexpr int kPend2Off = kPendOff + kStages * 16;              // int4 [kStages]: flags, buffer, item
     static constexpr int kItemOff = kPend2Off + kStages * 16;              // int4 [kMaxCtaItems]
     static constexpr int kBarOff = kItemOff + kMaxCtaItems * 16;
-    // full, empty, staged [kStages]; accum_full, accum_empty [2]; 4 flags, TMEM slot
-    static constexpr int kSmem = kBarOff + (3 * kStages + 4) * 8 + 24;
+    // full, empty, staged [kStages]; accum_full, accum_empty [2]; drain; 4 flags, TMEM slot
+    static constexpr int kSmem = kBarOff + (3 * kStages + 5) * 8 + 24;
     static_assert(kSmem <= 227 * 1024, "shared memory budget");
     static_assert(kStage % 1024 == 0 && kATileBytes % 1024 == 0, "swizzled tiles need 1024-byte alignment");
     static_assert(kStagingOff % 16 == 0 && kStagingBytes % 16 == 0 && kPendOff % 16 == 0, "16-byte alignment");
@@ -223,8 +223,9 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     uint64_t *staged = empty + S;
     uint64_t *acc_full = staged + S;  // [2]
     uint64_t *acc_empty = acc_full + 2; // [2]
-    volatile int *flag = reinterpret_cast<volatile int *>(acc_empty + 2); // 2 slots per scatter group
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + 2) + 4;
+    uint64_t *drain = acc_empty + 2;    // the MMA lane's last commit: every MMA it issued has completed
+    volatile int *flag = reinterpret_cast<volatile int *>(drain + 1); // 2 slots per scatter group
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1) + 4;
     constexpr int kScatterGroups = S % 2 == 0 ? 2 : 1; // two groups need an even ring (see the scatter role)
     constexpr int kGroupThreads = kScatterThreads / kScatterGroups;
 
@@ -251,6 +252,7 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             mbar_init(&acc_full[b], 1);
             mbar_init(&acc_empty[b], kEpiThreads);
         }
+        mbar_init(drain, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if ((int)threadIdx.x < n_items)
@@ -404,6 +406,9 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_f16(NT); // E4M3 has format code 0 in kind::f8f6f4 as FP16 in kind::f16
+            // test hook: the CTA's last accumulator is never announced, so the
+            // epilogue's bounded wait for it runs out (TCA_FLAG_TEST_WITHHOLD_ACCUM)
+            const bool withhold = (batch.job[0].flags & TCA_FLAG_TEST_WITHHOLD_ACCUM) != 0;
             for (int g = 0; g < total_chunks; g++) {
                 const int s = g % S;
                 if (!mbar_wait(&full[s], (g / S) & 1)) { ok = false; break; }
@@ -431,9 +436,14 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                     }
                 }
                 umma_commit(&empty[s]);
-                if (f.x & 2)
+                if ((f.x & 2) && !(withhold && k == n_items - 1))
                     umma_commit(&acc_full[b]);
             }
+            // every MMA issued has completed before the tensor memory is
+            // released, also when a role gave up early
+            umma_commit(drain);
+            if (!mbar_wait(drain, 0))
+                ok = false;
         }
         __syncwarp();
     } else {
@@ -490,10 +500,21 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         }
     }
 
-    if (!ok && n_items > 0)
-        atomicOr(batch.job[items[0].w >> 16].status, kStatusTimeout);
     tc_fence_before();
-    __syncthreads();
+    if (__syncthreads_or(!ok)) {
+        // A role gave up after a bounded wait: record it, then give bulk
+        // copies that loaders issued and nobody consumed a bounded time
+        // (1 ms; a copy lands within microseconds) to land before this
+        // CTA's shared memory is released.
+        if (threadIdx.x == 0) {
+            if (n_items > 0)
+                atomicOr(batch.job[items[0].w >> 16].status, kStatusTimeout);
+            const uint64_t t0 = global_ns();
+            while (global_ns() - t0 < 1000000ull) {
+            }
+        }
+        __syncthreads();
+    }
     if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * NT) : "memory");

@@ -112,6 +112,8 @@ _SIGS = {
                       ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP)], _I),
     "tca_free": ([_VP], None),
     "tca_spmm_host": ([_P, _P, _P, _I, _I, _I, _P, _I, _P, _I, _U, _I, ctypes.POINTER(ctypes.c_double)], _I),
+    "tca_pool_stats": ([_I, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+                        ctypes.POINTER(ctypes.c_size_t)], _I),
 }
 
 
@@ -134,6 +136,14 @@ def lib() -> ctypes.CDLL:
             fn.restype = res
         _lib = handle
     return _lib
+
+
+def pool_stats(reset_high: bool = False) -> dict:
+    """The library's device memory pool on the current device (tca_pool_stats):
+    bytes reserved, in use, and the highest use since the last reset."""
+    r, u, h = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_size_t()
+    _check(lib().tca_pool_stats(1 if reset_high else 0, ctypes.byref(r), ctypes.byref(u), ctypes.byref(h)))
+    return {"reserved": r.value, "used": u.value, "used_high": h.value}
 
 
 def _check(rc: int) -> None:

@@ -131,10 +131,13 @@ def test_reference_style_driver_compiles_and_links(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case,N", [(0, 256), (1, 64), (2, 320)])
+@pytest.mark.parametrize("case,N", [(0, 256), (1, 64), (2, 320), ("body_decoder_layer_2_ffn_conv1", 256)])
 def test_reference_style_driver_runs(tmp_path, cuda, case, N):
+    """The reference harness's flow on the seeded smtx files and on the
+    reference's own data fixture (the input its README runs)."""
     exe = _build_driver(tmp_path / "spmm_driver")
-    r = subprocess.run([str(exe), str(GOLD / f"smtx_{case}.smtx"), str(N)], capture_output=True, text=True,
+    name = f"smtx_{case}.smtx" if isinstance(case, int) else f"{case}.smtx"
+    r = subprocess.run([str(exe), str(GOLD / name), str(N)], capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "our: [" in r.stdout

@@ -6,6 +6,8 @@ product of absolute values, i.e. the scale of the FP32 rounding error):
   FP32 output: |C - C64| <= 1e-5 * S
   FP16 output: |C - C64| <= 1e-3 * |C64| + 1e-5 * S + 2**-24
 """
+import pathlib
+
 import numpy as np
 import pytest
 
@@ -225,7 +227,8 @@ def test_malformed_csr_is_rejected(cuda):
 
 
 # ------------------------------------------------------------------ full sizes
-@pytest.mark.parametrize("cfg", ["cfg1", "sweep80", "sweep98", "sweep70_512", "sweep90_64"])
+@pytest.mark.parametrize("cfg", ["cfg1", "sweep80", "sweep95", "sweep98", "sweep70_512", "sweep90_64",
+                                 "sweep80_128", "sweep95_128"])
 def test_full_size_configs(cuda, cfg):
     if cfg == "cfg1":
         c = gen.cfg1()
@@ -250,13 +253,27 @@ def test_host_api_reference_semantics(cuda):
 
 
 # ------------------------------------------------------------------ reference kernels
+def fixture_case():
+    """The reference's own data fixture (pattern only: every value 1.0), with
+    B as its harness makes it (src/test.cu:56: nonzero with probability 0.9,
+    value U(0, 1)), seeded, N = 256."""
+    path = pathlib.Path(__file__).resolve().parent / "golden" / "body_decoder_layer_2_ffn_conv1.smtx"
+    M, K, nnz, rp, ci = oracle.smtx_parse(path.read_bytes())
+    rng = np.random.default_rng(56)
+    B = np.where(rng.random((K, 256)) > 0.1, rng.random((K, 256)), 0.0).astype(np.float16)
+    return {"M": M, "K": K, "row_ptr": rp, "col": ci, "vals": np.ones(nnz, np.float16), "B": B}
+
+
 @pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("cfg", ["cfg1", "sweep80", "sweep98"])
+@pytest.mark.parametrize("cfg", ["cfg1", "sweep80", "sweep95", "sweep98", "fixture"])
 def test_matches_reference_tca_and_cusparse(cuda, cfg):
     """Our forward vs the reference's own our_spmm_balanced and its cuSPARSE
     comparator on the same inputs: within 1e-2 relative (compare_mat rule and
     relative Frobenius)."""
-    c = gen.cfg1() if cfg == "cfg1" else gen.sweep(int(cfg[5:]) / 100, N=256)
+    if cfg == "fixture":
+        c = fixture_case()
+    else:
+        c = gen.cfg1() if cfg == "cfg1" else gen.sweep(int(cfg[5:]) / 100, N=256)
     rp, ci, v, B = dev(c, cuda)
     plan = tca_spmm.Plan(rp, ci, v, c["K"])
     ours = plan.spmm(B, out_dtype=torch.float32).cpu().numpy()
@@ -286,4 +303,4 @@ def test_matches_reference_tca_and_cusparse(cuda, cfg):
     assert bad_short == 0  # its short-row path agrees with ours element by element
     if ref_err < 1e-2:
         assert rel(ours, ref_tca) < 1e-2
-    assert our_err < ref_err
+    assert our_err < ref_err or our_err < 1e-6
