@@ -9,16 +9,12 @@
 // entries are sorted by the 64-bit key (column, original row) with a stable
 // radix sort, so A^T's CSR -- and hence its plan -- is deterministic.
 //
-// dA has two paths. Dense-masked: D = dY B^T (M x K, FP32) as one cuBLAS GEMM
-// on the tensor cores (FP16 in, FP32 accumulation), then the nonzeros' entries
-// gathered from D -- it computes 1/density times the useful products but
-// reads dY and B once. Sparse: a warp per row streams the row of dY against
-// the B rows of its nonzeros, reading B once per nonzero (L2-bound). The
-// dense path is taken where its estimated time is lower (density above
-// ~0.004 + 1.5 / N, from the tensor-core rate against the L2 rate of the
-// sparse path) and D fits in kSddmmDenseMaxBytes of scratch.
+// dA on the tensor-core windows is a tcgen05 kernel of its own
+// (sddmm_tc.cu): per window and chunk the tile dY[window rows] B[chunk
+// columns]^T, of which the epilogue writes the nonzeros. The rows of the
+// CUDA-core windows (too sparse for tiles) take a warp per row that streams
+// the row of dY against the B rows of its nonzeros (L2-bound).
 #include <cub/cub.cuh>
-#include <cublas_v2.h>
 #include <vector>
 #include "tca_internal.cuh"
 #include "plan.cuh"
@@ -68,50 +64,6 @@ __global__ void k_scatter_half(const int *__restrict__ idx, const __half *__rest
         dst[idx[i]] = src[i];
 }
 
-// out[src[j]] = alpha * D[perm[i], p_col[j]] for the nonzeros j of sorted row
-// i: the dense-masked SDDMM's sampling step (one warp per row).
-template <typename OutT>
-__global__ void __launch_bounds__(256)
-k_sddmm_gather(const int *__restrict__ perm, const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
-               const int *__restrict__ src, int M, const float *__restrict__ D, int K, OutT *__restrict__ out,
-               float alpha)
-{
-    const int lane = threadIdx.x & 31;
-    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= M)
-        return;
-    const float *d = D + (size_t)perm[i] * K;
-    for (int j = p_row_ptr[i] + lane; j < p_row_ptr[i + 1]; j += 32) {
-        const float r = alpha * d[p_col[j]];
-        if constexpr (sizeof(OutT) == 2)
-            out[src[j]] = __float2half_rn(r);
-        else
-            out[src[j]] = r;
-    }
-}
-
-constexpr size_t kSddmmDenseMaxBytes = size_t(256) << 20; // D of the dense-masked SDDMM
-
-// This host thread's cuBLAS handle on the current device.
-int cublas_handle(cublasHandle_t *out)
-{
-    thread_local std::vector<std::pair<int, cublasHandle_t>> handles;
-    int dev = 0;
-    TCA_CUDA_TRY(cudaGetDevice(&dev));
-    for (const auto &h : handles)
-        if (h.first == dev) {
-            *out = h.second;
-            return TCA_OK;
-        }
-    cublasHandle_t h = nullptr;
-    const cublasStatus_t st = cublasCreate(&h);
-    if (st != CUBLAS_STATUS_SUCCESS)
-        return set_error(TCA_ERR_CUDA, "cublasCreate failed: %s", cublasGetStatusString(st));
-    handles.emplace_back(dev, h);
-    *out = h;
-    return TCA_OK;
-}
-
 __global__ void k_gather_half(const int *__restrict__ idx, const __half *__restrict__ src, __half *__restrict__ dst,
                               int n)
 {
@@ -120,19 +72,32 @@ __global__ void k_gather_half(const int *__restrict__ idx, const __half *__restr
         dst[i] = src[idx[i]];
 }
 
+// Sorted row of warp w: w itself, or with a window list (the CUDA-core
+// windows) row w % 128 of window windows[w / 128]; -1 past the rows.
+__device__ __forceinline__ long long sddmm_row(long long w, const int *windows, long long n_rows, int M)
+{
+    if (w >= n_rows)
+        return -1;
+    if (!windows)
+        return w;
+    const long long i = (long long)windows[w >> 7] * 128 + (w & 127);
+    return i < M ? i : -1;
+}
+
 // SDDMM, vectorised (N % 8 == 0, 16-byte aligned rows): one warp per sorted
 // row; 8 nonzeros in flight per lane, each lane covering 8 columns of every
 // 256-column slice; a warp-wide reduction per nonzero.
 template <typename OutT>
 __global__ void __launch_bounds__(256)
 k_sddmm_vec(const int *__restrict__ perm, const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
-            const int *__restrict__ src, int M, const __half *__restrict__ dY, int ldy,
-            const __half *__restrict__ B, int ldb, int N, OutT *__restrict__ out, float alpha)
+            const int *__restrict__ src, int M, const int *__restrict__ windows, long long n_rows,
+            const __half *__restrict__ dY, int ldy, const __half *__restrict__ B, int ldb, int N,
+            OutT *__restrict__ out, float alpha)
 {
     constexpr int U = 8;
     const int lane = threadIdx.x & 31;
-    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= M)
+    const long long i = sddmm_row(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5, windows, n_rows, M);
+    if (i < 0)
         return;
     const __half *y = dY + (size_t)perm[i] * ldy;
     const int j0 = p_row_ptr[i], j1 = p_row_ptr[i + 1];
@@ -183,12 +148,13 @@ k_sddmm_vec(const int *__restrict__ perm, const int *__restrict__ p_row_ptr, con
 template <typename OutT>
 __global__ void __launch_bounds__(256)
 k_sddmm_scalar(const int *__restrict__ perm, const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
-               const int *__restrict__ src, int M, const __half *__restrict__ dY, int ldy,
-               const __half *__restrict__ B, int ldb, int N, OutT *__restrict__ out, float alpha)
+               const int *__restrict__ src, int M, const int *__restrict__ windows, long long n_rows,
+               const __half *__restrict__ dY, int ldy, const __half *__restrict__ B, int ldb, int N,
+               OutT *__restrict__ out, float alpha)
 {
     const int lane = threadIdx.x & 31;
-    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= M)
+    const long long i = sddmm_row(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5, windows, n_rows, M);
+    if (i < 0)
         return;
     const __half *y = dY + (size_t)perm[i] * ldy;
     for (int j = p_row_ptr[i]; j < p_row_ptr[i + 1]; j++) {
@@ -314,42 +280,24 @@ int tca_sddmm(tca_plan_t plan, const void *d_dY_f16, int ldy, const void *d_B_f1
         return TCA_OK;
     }
     const __half *y = (const __half *)d_dY_f16, *b = (const __half *)d_B_f16;
-    const unsigned grid = blocks_of((long long)plan->M * 32, 256);
-    const double density = (double)plan->nnz / ((double)plan->M * (double)plan->K);
-    const size_t d_bytes = sizeof(float) * (size_t)plan->M * (size_t)plan->K;
-    if (density > 0.004 + 1.5 / N && d_bytes <= kSddmmDenseMaxBytes) {
-        // D (row-major M x K) = dY B^T, i.e. column-major D^T = B dY^T:
-        // B row-major K x N is column-major N x K (transposed: op T), dY
-        // row-major M x N is column-major N x M (op N)
-        cublasHandle_t h = nullptr;
-        TCA_TRY(cublas_handle(&h));
-        float *D = nullptr;
-        TCA_TRY(dev_malloc((void **)&D, d_bytes, s));
-        const float one = 1.f, zero = 0.f;
-        cublasStatus_t cs = cublasSetStream(h, s);
-        if (cs == CUBLAS_STATUS_SUCCESS)
-            cs = cublasGemmEx(h, CUBLAS_OP_T, CUBLAS_OP_N, plan->K, plan->M, N, &one, b, CUDA_R_16F, ldb, y,
-                              CUDA_R_16F, ldy, &zero, D, CUDA_R_32F, plan->K, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-        if (cs != CUBLAS_STATUS_SUCCESS) {
-            dev_free(D, s);
-            return set_error(TCA_ERR_CUDA, "cublasGemmEx (dY B^T) failed: %s", cublasGetStatusString(cs));
-        }
-        if (out_dtype == TCA_DTYPE_F16)
-            k_sddmm_gather<__half><<<grid, 256, 0, s>>>(plan->perm, plan->p_row_ptr, plan->p_col, plan->src, plan->M,
-                                                        D, plan->K, (__half *)d_out, alpha);
-        else
-            k_sddmm_gather<float><<<grid, 256, 0, s>>>(plan->perm, plan->p_row_ptr, plan->p_col, plan->src, plan->M,
-                                                       D, plan->K, (float *)d_out, alpha);
-        const cudaError_t e = cudaGetLastError();
-        dev_free(D, s);
-        if (e != cudaSuccess)
-            return set_error(TCA_ERR_CUDA, "k_sddmm_gather launch failed: %s", cudaGetErrorString(e));
-        return TCA_OK;
+    // the tensor-core windows on the tensor cores (TMA needs 16-byte aligned
+    // rows), then the rows the CUDA-core kernels cover: those of the
+    // CUDA-core windows, or every row
+    const bool tma_ok = ldy % 8 == 0 && ldb % 8 == 0 && aligned16(y) && aligned16(b);
+    const int *windows = nullptr;
+    long long n_rows = plan->M;
+    if (plan->n_tc > 0 && tma_ok) {
+        TCA_TRY(sddmm_tc(plan, y, ldy, b, ldb, N, d_out, out_dtype == TCA_DTYPE_F16, alpha, s));
+        windows = plan->cc_windows;
+        n_rows = (long long)plan->n_cc * kWindowRows;
     }
+    if (n_rows == 0)
+        return TCA_OK;
+    const unsigned grid = blocks_of(n_rows * 32, 256);
     const bool vec = (N % 8 == 0) && (ldy % 8 == 0) && (ldb % 8 == 0) && aligned16(y) && aligned16(b);
 #define TCA_SDDMM(KERN, T)                                                                                  \
-    KERN<T><<<grid, 256, 0, s>>>(plan->perm, plan->p_row_ptr, plan->p_col, plan->src, plan->M, y, ldy, b, ldb, N, \
-                                 (T *)d_out, alpha)
+    KERN<T><<<grid, 256, 0, s>>>(plan->perm, plan->p_row_ptr, plan->p_col, plan->src, plan->M, windows, n_rows, y, \
+                                 ldy, b, ldb, N, (T *)d_out, alpha)
     if (vec) {
         if (out_dtype == TCA_DTYPE_F16) TCA_SDDMM(k_sddmm_vec, __half);
         else TCA_SDDMM(k_sddmm_vec, float);

@@ -241,6 +241,95 @@ __global__ void __launch_bounds__(256) k_quant_cols(const __grid_constant__ QBat
     }
 }
 
+// The whole quantization of B in one launch: one block per (matrix, strip of
+// SW columns) reads the strip's K rows for the column maxima, reduces them
+// (warp shuffles, then the block's 8 warps), writes the scales and reads the
+// strip again (now from L2) to quantize it. Nothing is cleared beforehand
+// and no block depends on another. A thread takes 8 consecutive columns
+// (16 bytes) of every RPP-th row, four rows' loads in flight.
+template <int SW>
+__global__ void __launch_bounds__(256) k_quant_b_strip(const __grid_constant__ QBatch b)
+{
+    constexpr int TPR = SW / 8;    // threads per row
+    constexpr int RPP = 256 / TPR; // rows per pass
+    const QJob &q = b.job[blockIdx.y];
+    const int n0 = blockIdx.x * SW;
+    if (n0 >= q.N)
+        return; // whole block
+    __shared__ float s_m[8][SW];
+    __shared__ float s_scale[SW];
+    const int tx = threadIdx.x % TPR, ty = threadIdx.x / TPR;
+    const int n = n0 + tx * 8;
+    const bool vec = vec8_ok(q);
+    float m[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (n < q.N) {
+        for (int k = ty; k < q.K; k += 4 * RPP) {
+            float v[4][8];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (k + u * RPP < q.K)
+                    load8h(q, k + u * RPP, n, vec, v[u]);
+                else
+#pragma unroll
+                    for (int i = 0; i < 8; i++) v[u][i] = 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int i = 0; i < 8; i++) m[i] = fmaxf(m[i], fabsf(v[u][i]));
+        }
+    }
+    // lanes of a warp with the same columns differ by multiples of TPR
+#pragma unroll
+    for (int o = TPR; o < 32; o <<= 1)
+#pragma unroll
+        for (int i = 0; i < 8; i++) m[i] = fmaxf(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane < TPR)
+#pragma unroll
+        for (int i = 0; i < 8; i++) s_m[warp][lane * 8 + i] = m[i];
+    __syncthreads();
+    if ((int)threadIdx.x < SW) {
+        float v = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; w++) v = fmaxf(v, s_m[w][threadIdx.x]);
+        const float sc = scale_of(v);
+        s_scale[threadIdx.x] = sc;
+        if (n0 + (int)threadIdx.x < q.N)
+            q.colmax[n0 + threadIdx.x] = __float_as_uint(sc);
+    }
+    __syncthreads();
+    if (n >= q.N)
+        return;
+    float sc[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) sc[i] = s_scale[tx * 8 + i];
+    const bool st8 = n + 8 <= q.N && (q.ldq & 7) == 0 && (reinterpret_cast<uintptr_t>(q.Bq) & 7u) == 0;
+    for (int k = ty; k < q.K; k += 4 * RPP) {
+        float v[4][8];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (k + u * RPP < q.K)
+                load8h(q, k + u * RPP, n, vec, v[u]);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (k + u * RPP >= q.K)
+                break;
+            uint32_t lo = 0, hi = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                lo |= (uint32_t)to_e4m3(v[u][i] / sc[i]) << (8 * i);
+                hi |= (uint32_t)to_e4m3(v[u][4 + i] / sc[4 + i]) << (8 * i);
+            }
+            uint8_t *dst = q.Bq + (size_t)(k + u * RPP) * q.ldq + n;
+            if (st8)
+                *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
+            else
+                for (int i = 0; n + i < q.N && i < 8; i++) dst[i] = (uint8_t)((i < 4 ? lo : hi) >> (8 * (i & 3)));
+        }
+    }
+}
+
 // column maxima -> scales, in place
 __global__ void k_col_scale(const __grid_constant__ QBatch b)
 {
@@ -261,6 +350,23 @@ int quantize_b_batch(const QBatch &b, cudaStream_t s)
     if (b.n == 0 || maxK == 0 || maxN == 0)
         return TCA_OK;
     const unsigned z = (unsigned)b.n;
+    // One launch, a block per column strip (k_quant_b_strip), when the strips
+    // give about two blocks per SM; else (few, wide matrices) the column
+    // maxima of 64-row tiles with one atomic per column and block, then the
+    // quantization and the scales, in four launches.
+    auto strips = [&](int sw) { return (long long)b.n * blocks(maxN, sw); };
+    if (strips(8) >= kSMs) {
+        const int sw = strips(64) >= 2 * kSMs ? 64 : strips(32) >= 2 * kSMs ? 32 : strips(16) >= 2 * kSMs ? 16 : 8;
+        const dim3 grid(blocks(maxN, sw), z);
+        switch (sw) {
+        case 64: k_quant_b_strip<64><<<grid, 256, 0, s>>>(b); break;
+        case 32: k_quant_b_strip<32><<<grid, 256, 0, s>>>(b); break;
+        case 16: k_quant_b_strip<16><<<grid, 256, 0, s>>>(b); break;
+        default: k_quant_b_strip<8><<<grid, 256, 0, s>>>(b); break;
+        }
+        TCA_CUDA_TRY(cudaGetLastError());
+        return TCA_OK;
+    }
     const dim3 tiles(blocks(maxN, kQTileCols), blocks(maxK, kQTileRows), z), tile_threads(32, 8);
     if (tiles.y > 65535u)
         return set_error(TCA_ERR_INVALID_ARG, "B has too many rows to quantize (K=%d)", maxK);
@@ -353,7 +459,7 @@ int make_fp8_job(tca_plan_t p, const void *B, int ldb, int N, void *C, int ldc, 
     job->ldc = ldc;
     job->f8 = true;
     job->tc = p->n_tc > 0;
-    job->n_tile = pick_tc_tile(p->n_tc, N, batched, true);
+    job->n_tile = pick_tc_tile(p, N, batched, true);
     if (p->M == 0 || N == 0 || p->K == 0)
         return TCA_OK;
     uint8_t *Bq;
@@ -558,11 +664,12 @@ int tca_spmm_fp8_static(tca_plan_t p, const void *d_B_f16, int ldb, int N, void 
     job.ldc = ldc;
     job.f8 = true;
     job.tc = p->n_tc > 0;
-    job.n_tile = pick_tc_tile(p->n_tc, N, false, true);
+    job.n_tile = pick_tc_tile(p, N, false, true, false);
     job.Bq = Bq;
     job.ldq = ldq;
     job.col_scale = scale;
-    // the same launches as tca_spmm_fp8 (the CUDA-core launch runs beside the
-    // tensor-core launch as its programmatic dependent); they allocate nothing
-    return run_jobs_with_events(&job, 1, c_dtype, alpha, beta, flags, s, nullptr);
+    // the launches of tca_spmm_fp8 (the CUDA-core launch runs beside the
+    // tensor-core launch as its programmatic dependent), with every item run
+    // whole on one CTA: nothing to allocate for split items
+    return run_jobs_with_events(&job, 1, c_dtype, alpha, beta, flags, s, nullptr, true);
 }

@@ -557,6 +557,7 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     p->n_tc = (int)tc_list.size();
     p->n_cc = (int)cc_list.size();
     p->n_tc_chunks = h_first.back();
+    p->h_tile_first = h_first;
     p->tc_nnz = ebase;
     TCA_TRY(dev_alloc(&p->tc_windows, p->n_tc, bytes));
     TCA_TRY(dev_alloc(&p->cc_windows, p->n_cc, bytes));
@@ -655,13 +656,14 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
 
 namespace tca {
 int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                         cudaStream_t s, void *const *events)
+                         cudaStream_t s, void *const *events, bool no_alloc)
 {
     // Without events the CUDA-core launches follow the tensor-core launch as
     // programmatic dependents and run beside it; with events (which time each
     // path alone) the two run one after the other.
     LaunchList tc, cc;
-    TCA_TRY(launch_tc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &tc));
+    TcWorkspace ws;
+    TCA_TRY(launch_tc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &tc, no_alloc ? nullptr : &ws));
     int beside = 0;
     for (int i = 0; !events && !tc.empty() && i < n_jobs; i++) {
         int r = 0;
@@ -672,20 +674,36 @@ int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alp
     // Under stream capture a plain record only orders the graph; an external
     // record becomes a graph node that records the event at every replay.
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    if (events)
-        TCA_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
-    const unsigned rec_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+    TCA_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
+    const bool capturing = cap == cudaStreamCaptureStatusActive;
+    // the split launches' workspace, for this call only: arrival counters
+    // (cleared) then partial tiles; under capture it becomes the graph's own
+    // memory (cudaMallocAsync), otherwise it comes from the library's pool
+    void *wsp = nullptr;
+    if (ws.partial_bytes > 0) {
+        const size_t head = (sizeof(int) * kArrivalSlots + 255) & ~(size_t)255;
+        if (capturing)
+            TCA_CUDA_TRY(cudaMallocAsync(&wsp, head + ws.partial_bytes, s));
+        else
+            TCA_TRY(dev_malloc(&wsp, head + ws.partial_bytes, s));
+        ws.arrivals = static_cast<int *>(wsp);
+        ws.partials = reinterpret_cast<float *>(static_cast<char *>(wsp) + head);
+        TCA_CUDA_TRY(cudaMemsetAsync(ws.arrivals, 0, sizeof(int) * kArrivalSlots, s));
+    }
+    const unsigned rec_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     auto rec = [&](int i) -> int {
         if (events && events[i]) TCA_CUDA_TRY(cudaEventRecordWithFlags((cudaEvent_t)events[i], s, rec_flags));
         return TCA_OK;
     };
-    TCA_TRY(rec(0));
-    for (auto &f : tc) TCA_TRY(f(s));
-    TCA_TRY(rec(1));
-    TCA_TRY(rec(2));
-    for (auto &f : cc) TCA_TRY(f(s));
-    TCA_TRY(rec(3));
-    return TCA_OK;
+    int st = rec(0);
+    for (size_t i = 0; st == TCA_OK && i < tc.size(); i++) st = tc[i](s);
+    if (st == TCA_OK) st = rec(1);
+    if (st == TCA_OK) st = rec(2);
+    for (size_t i = 0; st == TCA_OK && i < cc.size(); i++) st = cc[i](s);
+    if (st == TCA_OK) st = rec(3);
+    if (wsp)
+        cudaFreeAsync(wsp, s); // after every launch of the call in stream order
+    return st;
 }
 } // namespace tca
 
@@ -840,7 +858,7 @@ static int make_job(tca_plan_t p, const void *d_B_f16, int ldb, int N, void *d_C
     job->N = N;
     job->ldc = ldc;
     job->tc = p->n_tc > 0 && dense_operands_vec_ok(d_B_f16, ldb, N, d_C, ldc, c_dtype);
-    job->n_tile = pick_tc_tile(p->n_tc, N, batched);
+    job->n_tile = pick_tc_tile(p, N, batched);
     return TCA_OK;
 }
 

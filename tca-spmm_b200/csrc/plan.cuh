@@ -59,6 +59,9 @@ struct tca_plan {
     int2 *cc_items = nullptr;
     int2 *all_items = nullptr;
     int n_cc_items = 0, n_all_items = 0;
+    // host copy of tile_first: chunk offsets of the tensor-core windows
+    // (n_tc + 1), for sizing the launches' chunk ranges
+    std::vector<int> h_tile_first;
     int *d_status = nullptr; // device error word written by bounded waits
     size_t bytes = 0;
     // A^T as a plan of its own (built on first use by tca_spmm_t or by
@@ -112,6 +115,7 @@ constexpr int kMaxTcK = 1 << 17;
 // Device status bits.
 constexpr int kStatusTimeout = 1;
 constexpr int kStatusLayout = 2; // shared memory base not 1024-byte aligned: the kernel did no work
+constexpr int kStatusTable = 4;  // a CTA's chunk range held more items than its work table: work was left out
 
 // One forward of one plan, as the batched launchers see it.
 struct SpmmJob {
@@ -134,11 +138,26 @@ struct SpmmJob {
 // descriptors) is already done: running one only launches.
 using LaunchList = std::vector<std::function<int(cudaStream_t)>>;
 
+// Device workspace of the tensor-core launches of one call whose work is
+// split across CTAs by chunk ranges: the arrival counters (zero before the
+// first launch; the launches leave them zero) and the partial tiles. The
+// caller allocates partial_bytes (as reported by launch_tc_jobs) before
+// running the deferred launches.
+struct TcWorkspace {
+    size_t partial_bytes = 0;
+    float *partials = nullptr;
+    int *arrivals = nullptr;
+};
+constexpr int kArrivalSlots = 2 * kSMs;
+
 // Tensor-core (tcgen05) forward over the tensor-core windows of every job
 // (jobs with tc set), in as few launches as the N-slice widths allow. With
-// `defer` the prepared launches are appended to it instead of issued.
+// `defer` the prepared launches are appended to it instead of issued. With a
+// workspace, launches split their work across CTAs by chunk ranges where
+// that fits (and record the partial-tile bytes they need in it); without,
+// every item runs whole on one CTA (nothing to allocate).
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s, LaunchList *defer = nullptr);
+                   cudaStream_t s, LaunchList *defer, TcWorkspace *ws);
 
 // Registers that one block of the tensor-core kernel holds on an SM (the
 // largest over its FP16 or its E4M3 instantiations).
@@ -158,12 +177,22 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
 // CUDA-core launches, so that the events bracket device work only. Without
 // events, the CUDA-core launches run concurrently with the tensor-core launch
 // (programmatic dependents on the same stream; the two paths write disjoint
-// rows of C).
+// rows of C). The tensor-core work is split across CTAs by chunk ranges, with
+// a workspace allocated on the stream for the call (stream-ordered, so calls
+// on different streams never share one); no_alloc: nothing is allocated and
+// items run whole.
 int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                         cudaStream_t s, void *const *events);
+                         cudaStream_t s, void *const *events, bool no_alloc = false);
 
-// The N-slice width a single forward of this plan uses.
-int pick_tc_tile(int n_tc, int N, bool batched, bool f8 = false);
+// The N-slice width a single forward of this plan uses (split: the launch
+// cuts items by chunk ranges).
+int pick_tc_tile(const tca_plan *p, int N, bool batched, bool f8 = false, bool split = true);
+
+// SDDMM over the plan's tensor-core windows on the tensor cores
+// (sddmm_tc.cu); dY and B with 16-byte aligned rows. The nonzeros of the
+// CUDA-core windows are left to the caller.
+int sddmm_tc(const tca_plan *p, const __half *dY, int ldy, const __half *B, int ldb, int N, void *out, bool out_f16,
+             float alpha, cudaStream_t s);
 
 // E4M3 form of A (fp8.cu): refresh after new values (when it exists); release.
 int plan_requantize_fp8(tca_plan *p, cudaStream_t s);

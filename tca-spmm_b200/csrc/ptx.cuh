@@ -65,6 +65,19 @@ __device__ __forceinline__ void named_bar_sync(int id, int n)
 {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
+// Named barrier that also returns the AND of `pred` over the n threads.
+__device__ __forceinline__ bool named_bar_and(int id, int n, bool pred)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred p, q;\n\t"
+                 "setp.ne.u32 p, %1, 0;\n\t"
+                 "bar.red.and.pred q, %2, %3, p;\n\t"
+                 "selp.u32 %0, 1, 0, q;\n\t}\n"
+                 : "=r"(r)
+                 : "r"((uint32_t)pred), "r"(id), "r"(n)
+                 : "memory");
+    return r != 0;
+}
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 

@@ -99,6 +99,19 @@ def test_fp8_forward_vs_dequantized_f64(cuda, case, path, N, out_dtype):
     assert err <= (2e-5 if out_dtype == "f32" else 1e-3), err
 
 
+@pytest.mark.parametrize("K,N", [(300, 2048), (257, 2047), (64, 9472), (1024, 1184)])
+def test_b_quantization_one_launch_bit_exact(cuda, K, N):
+    """Wide B (enough column strips for the one-launch quantization, several
+    strip widths, a ragged last strip) against the oracle, bit for bit."""
+    rng = np.random.default_rng(K + N)
+    B = (rng.standard_normal((K, N)) * rng.choice([1e-3, 1.0, 50.0], N)).astype(np.float16)
+    B[:, 3] = 0  # an all-zero column: scale 1
+    Bq, sb = tca_spmm.quantize_b_fp8(torch.from_numpy(B).to(cuda))
+    qb, sb_ref = oracle.quant_cols(B, ldq=Bq.shape[1])
+    np.testing.assert_array_equal(sb.cpu().numpy().view(np.uint32), sb_ref.view(np.uint32))
+    np.testing.assert_array_equal(Bq.cpu().numpy()[:, :N], qb[:, :N])
+
+
 def test_fp8_alpha_beta_and_empty_rows(cuda):
     c = gen.small(np.random.default_rng(3), 500, 300, 64, 0.1, empty_rows=0.2)
     rp, ci, v, B = dev(c, cuda)

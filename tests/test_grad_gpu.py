@@ -49,6 +49,44 @@ def test_sddmm_and_transpose_small(cuda, N, path):
     plan.status()
 
 
+@pytest.mark.parametrize("M,K,N,d,path,out", [
+    (640, 4096, 256, 0.05, "auto", "f32"),        # 64 direct chunks a window: 8 chunk groups, n cut in parts
+    (400, 1024, 96, 0.3, "auto", "f16"),          # FP16 out; N not a multiple of 64 (zero-filled tail)
+    (1300, 20000, 64, 0.004, "tensor_core", "f32"),  # condensed chunks (gathered B rows), 11 windows
+    (2048, 512, 4096, 0.1, "auto", "f32"),        # the differentiation config's shape
+])
+def test_sddmm_tensor_core_windows(cuda, M, K, N, d, path, out):
+    """The tcgen05 SDDMM over tensor-core windows (and the CUDA-core rows
+    beside them) against the FP64 product, elementwise."""
+    rng = np.random.default_rng(M + K)
+    c = gen.small(rng, M, K, N, d, empty_rows=0.02)
+    dY = rng.standard_normal((M, N)).astype(np.float16)
+    plan = tca_spmm.Plan(dev(c["row_ptr"], cuda), dev(c["col"], cuda), dev(c["vals"], cuda), c["K"], path=path)
+    assert plan.info()["n_tc_windows"] > 0
+    dt = torch.float16 if out == "f16" else torch.float32
+    dA = plan.sddmm(dev(dY, cuda), dev(c["B"], cuda), out_dtype=dt).float().cpu().numpy()
+    dA2 = plan.sddmm(dev(dY, cuda), dev(c["B"], cuda), out_dtype=dt).float().cpu().numpy()
+    torch.cuda.synchronize()
+    plan.status()
+    rA = f64_grads(c, dY)[0]
+    # FP32 accumulation over N products of FP16 inputs; FP16 out adds half an ulp
+    scale = np.sqrt(N) * np.abs(rA).mean() + np.abs(rA)
+    tol = (1e-3 * np.abs(rA) if out == "f16" else 0) + 1e-5 * scale
+    assert np.all(np.abs(dA - rA) <= tol), np.abs(dA - rA).max()
+    assert np.array_equal(dA, dA2)  # the parts are added in a fixed order
+
+
+def test_sddmm_unaligned_rows_take_the_cuda_core_kernels(cuda):
+    rng = np.random.default_rng(5)
+    c = gen.small(rng, 300, 256, 100, 0.2)
+    wide = rng.standard_normal((300, 101)).astype(np.float16)
+    dY = dev(wide, cuda)[:, :100]  # row stride 101: not 16-byte aligned rows
+    plan = tca_spmm.Plan(dev(c["row_ptr"], cuda), dev(c["col"], cuda), dev(c["vals"], cuda), c["K"])
+    assert plan.info()["n_tc_windows"] > 0
+    dA = plan.sddmm(dY, dev(c["B"], cuda)).cpu().numpy()
+    assert rel(dA, f64_grads(c, wide[:, :100])[0]) < 1e-5
+
+
 def test_transpose_follows_value_updates(cuda):
     rng = np.random.default_rng(7)
     c = gen.small(rng, 200, 150, 64, 0.1)

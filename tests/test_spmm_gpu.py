@@ -243,6 +243,30 @@ def test_full_size_configs(cuda, cfg):
     plan.status()
 
 
+@pytest.mark.parametrize("M,K,N,d", [(256, 8192, 64, 0.3), (1000, 4096, 136, 0.2), (300, 2048, 512, 0.5)])
+def test_items_cut_across_ctas(cuda, M, K, N, d):
+    """Few windows with many chunks each: the launch cuts every item into
+    parts on several CTAs (chunk ranges), and the part that arrives last adds
+    the others' partial tiles in part order. FP32 and FP16 outputs within the
+    tolerances above, E4M3 within 2e-5 of the FP64 product of its dequantized
+    operands, and two launches identical bit for bit."""
+    c = gen.small(np.random.default_rng(M + K), M, K, N, d, empty_rows=0.05)
+    rp, ci, v, B = dev(c, cuda)
+    plan = tca_spmm.Plan(rp, ci, v, c["K"])
+    assert plan.info()["n_tc_windows"] > 0
+    C1 = plan.spmm(B, out_dtype=torch.float32)
+    C2 = plan.spmm(B, out_dtype=torch.float32)
+    torch.cuda.synchronize()
+    plan.status()
+    assert torch.equal(C1, C2)
+    assert_close(C1, c)
+    assert_close(plan.spmm(B, out_dtype=torch.float16), c)
+    C8 = plan.spmm_fp8(B, out_dtype=torch.float32).double().cpu().numpy()
+    ref8 = oracle.spmm_fp8_f64(c["row_ptr"], c["col"], c["vals"], c["B"])
+    assert np.linalg.norm(C8 - ref8) <= 2e-5 * np.linalg.norm(ref8)
+    plan.status()
+
+
 def test_host_api_reference_semantics(cuda):
     rng = np.random.default_rng(40)
     c = gen.small(rng, 500, 256, 64, 0.05, empty_rows=0.3)
