@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-per-problem", action="store_true", help="skip the per-problem comparison leg")
+    ap.add_argument("--only", choices=["step", "step_e4m3", "fwd_bwd", "batching", "e2e"], default=None,
+                    help="run only this leg (for profiling: ncu captures of one kernel); prints its own line")
     return ap.parse_args()
 
 
@@ -371,6 +373,40 @@ def run_ours(args, world, rank):
     return out, distinct
 
 
+def run_only(args, world):
+    """One leg alone, for profiling runs: the headline step (FP16 or E4M3)
+    replayed `steps` times after `warmup`, the differentiation config, the
+    batching config, or the host-buffer forward."""
+    import torch
+    import tca_spmm
+    if args.only == "fwd_bwd":
+        return fwd_bwd_leg(args, False)
+    if args.only == "batching":
+        return batching_leg(args, world)
+    distinct = make_problems(args)
+    if args.only == "e2e":
+        c = distinct[0]
+        t0 = time.perf_counter()
+        for _ in range(args.warmup + args.steps):
+            tca_spmm.spmm_host(c["row_ptr"], c["col"], c["vals"], c["K"], c["B"],
+                               C=np.empty((c["M"], args.n), np.float16), keep_empty_rows=False)
+        return {"s": time.perf_counter() - t0}
+    dev = torch.device("cuda", torch.cuda.current_device())
+    plans, Bs, Cs = [], [], []
+    for g in range(args.problems):
+        c = distinct[g % len(distinct)]
+        rp, ci, v, B = (torch.from_numpy(c[k]).to(dev) for k in ("row_ptr", "col", "vals", "B"))
+        plans.append(tca_spmm.Plan(rp, ci, v, c["K"]))
+        Bs.append(B)
+        Cs.append(torch.empty((c["M"], args.n), dtype=torch.float16, device=dev))
+    g = tca_spmm.BatchGraph(plans, Bs, Cs, precision="e4m3" if args.only == "step_e4m3" else "f16")
+    for _ in range(args.warmup + args.steps):
+        g.launch()
+    torch.cuda.synchronize()
+    g.close()
+    return {"problems": args.problems}
+
+
 def kernel_times(tca_spmm, torch, plans, Bs, Cs, precision, reps):
     """(tensor-core ms, CUDA-core ms) per replay of the batch captured in a
     CUDA graph with events around each kernel group."""
@@ -389,10 +425,26 @@ def kernel_times(tca_spmm, torch, plans, Bs, Cs, precision, reps):
     return tc, cc
 
 
+def graph_of(torch, fn):
+    """fn (launches on torch's current stream) captured once as a CUDA graph."""
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        fn()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s, capture_error_mode="relaxed"):
+        fn()
+    return g
+
+
 def batching_leg(args, world):
-    """The batching config: 24 layers of mixed shapes, sparsity and N, as one
-    autotuned batch replayed from a CUDA graph vs 24 sequential forwards
-    (tca_spmm per layer), device time per pass (CUDA events, median of runs)."""
+    """The batching config: 24 layers of mixed shapes, sparsity and N. Device
+    time per pass (CUDA events, median of runs) of: the autotuned batch
+    (tca_spmm_batched, one CUDA graph); the same batch with one configuration
+    for every layer (N slice 128, 8 CUDA-core columns a lane: the fewest
+    launches); and 24 sequential forwards (tca_spmm per layer), both eager and
+    captured as one CUDA graph of the 24 calls. Roofline: compulsory bytes of
+    the 24 layers over the batch's time."""
     import torch
     import tca_spmm
     from tca_spmm import gen
@@ -405,12 +457,16 @@ def batching_leg(args, world):
         Bs.append(torch.from_numpy(c["B"].copy()).to(dev))
         outs.append(torch.empty((c["M"], c["N"]), dtype=torch.float16, device=dev))
     flops = sum(2.0 * c["col"].size * c["N"] for c in ls)
+    nbytes = sum(problem_bytes(c, c["N"]) for c in ls)
     tuned = tca_spmm.autotune(plans, Bs, outs, reps=3)
     g = tca_spmm.BatchGraph(plans, Bs, outs, n_tiles=[t[0] for t in tuned], cc_cols=[t[1] for t in tuned])
+    g1 = tca_spmm.BatchGraph(plans, Bs, outs, n_tiles=[128] * len(ls), cc_cols=[8] * len(ls))
 
     def seq():
         for p, B, C in zip(plans, Bs, outs):
             p.spmm(B, out=C)
+
+    gseq = graph_of(torch, seq)
 
     def timed(fn, reps=20):
         for _ in range(3):
@@ -426,13 +482,30 @@ def batching_leg(args, world):
             ts.append(a.elapsed_time(b) * 1e3)
         return float(np.median(ts))
 
-    t_graph = timed(g.launch)
-    t_seq = timed(seq)
+    t_graph, t_one = timed(g.launch), timed(g1.launch)
+    t_seq_graph, t_seq = timed(gseq.replay), timed(seq)
     g.close()
+    g1.close()
+    peak, _ = peaks()
+
+    def launches(n_tiles, cc_cols):
+        """(tensor-core, CUDA-core) launches of one batched call."""
+        tc = {nt for p, nt in zip(plans, n_tiles) if p.info()["n_tc_windows"] > 0}
+        cc = {w for p, w in zip(plans, cc_cols) if p.info()["n_cc_windows"] > 0}
+        return len(tc), len(cc)
+
     return {"workload": "24 layers: 6 each of 512x2048, 2048x512, 512x512, 1024x4096; sparsity U[0.5, 0.98]; "
                         "N per layer from {64..1024}; FP16",
-            "graph_us": round(t_graph, 2), "sequential_us": round(t_seq, 2),
-            "speedup": round(t_seq / t_graph, 3), "graph_gflops": round(flops / (t_graph * 1e-6) / 1e9, 1),
+            "graph_us": round(t_graph, 2), "sequential_graph_us": round(t_seq_graph, 2),
+            "sequential_eager_us": round(t_seq, 2), "one_config_graph_us": round(t_one, 2),
+            "speedup_vs_sequential_graph": round(t_seq_graph / t_graph, 3),
+            "speedup_vs_sequential_eager": round(t_seq / t_graph, 3),
+            "launches": {"tuned": launches([t[0] for t in tuned], [t[1] for t in tuned]),
+                         "one_config": launches([128] * len(ls), [8] * len(ls)),
+                         "sequential": sum(sum(p.launch_counts(c["N"])) for p, c in zip(plans, ls))},
+            "graph_gflops": round(flops / (t_graph * 1e-6) / 1e9, 1),
+            "roofline_frac": round(nbytes / (t_graph * 1e-6) / 1e9 / peak, 4),
+            "compulsory_bytes": nbytes,
             "tuned": [list(t) for t in tuned]}
 
 
@@ -719,6 +792,9 @@ def main():
             return
         out, _ = run_reference(args, 1, 0)
         print(json.dumps(out), flush=True)
+        return
+    if args.only is not None:
+        print(json.dumps({"only": args.only, **run_only(args, world)}), flush=True)
         return
     out, distinct = run_ours(args, world, rank)
     if rank == 0:

@@ -82,15 +82,16 @@ __global__ void k_gather_int(const int *__restrict__ src, const int *__restrict_
         dst[i] = src[idx[i]];
 }
 
-// 2b. Re-order the CSR: one warp per sorted row.
+// 2b. Re-order the CSR: one warp per sorted row. Does nothing when the row
+// checks found an error (the host reports it after its next wait).
 __global__ void k_permute(const int *__restrict__ perm, const int *__restrict__ row_ptr,
                           const int *__restrict__ col, const __half *__restrict__ val,
-                          const int *__restrict__ p_row_ptr, int M, int *__restrict__ p_col,
-                          __half *__restrict__ p_val, int *__restrict__ src)
+                          const int *__restrict__ p_row_ptr, int M, const int *__restrict__ err,
+                          int *__restrict__ p_col, __half *__restrict__ p_val, int *__restrict__ src)
 {
     const int lane = threadIdx.x & 31;
     const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= M)
+    if (i >= M || *err)
         return;
     const int r = perm[i];
     const int s = row_ptr[r], e = row_ptr[r + 1], d = p_row_ptr[i];
@@ -129,13 +130,17 @@ __device__ __forceinline__ void mark_columns(const int *__restrict__ p_col, int 
 }
 
 // 3. Window statistics: one block per window, K-bit bitmap in shared memory.
+// Does nothing when the row checks found an error (see k_permute).
 __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
-                               const int *__restrict__ p_sorted, int M, int K, int *__restrict__ win_nu,
-                               int *__restrict__ win_nnz, int *__restrict__ win_elig, int *__restrict__ win_nblk)
+                               const int *__restrict__ p_sorted, int M, int K, const int *__restrict__ err,
+                               int *__restrict__ win_nu, int *__restrict__ win_nnz, int *__restrict__ win_elig,
+                               int *__restrict__ win_nblk)
 {
     extern __shared__ uint32_t bm[];
     __shared__ int s_cnt, s_elig, s_nblk;
     const int w = blockIdx.x;
+    if (*err)
+        return; // uniform across the block
     const int nwords = (K + 31) >> 5;
     for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
     if (threadIdx.x == 0) { s_cnt = 0; s_elig = 1; s_nblk = 0; }
@@ -433,7 +438,11 @@ void build_items(const std::vector<int> &windows, const std::vector<int> &row_pt
     }
 }
 
-int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *val, cudaStream_t s)
+// vals_ready: an event after which `val` may be read (the host-buffer path
+// copies the values on a second stream); sync_end: wait for the whole build
+// before returning (so that the plan is usable on any stream).
+int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *val, cudaStream_t s,
+               cudaEvent_t vals_ready = nullptr, bool sync_end = true)
 {
     BuildStream build_stream(s);
     const int M = p->M, K = p->K, nnz = p->nnz;
@@ -457,25 +466,24 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     TCA_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, sizeof(int), s));
     TCA_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
 
-    // 1. checks
+    // 1. checks; the host reads their verdict with the window statistics
+    // (step 3), the kernels that follow stand down on an error
     k_row_check<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(row_ptr, col, M, K, nnz, row_nnz, row_sorted, err);
     TCA_CUDA_TRY(cudaGetLastError());
-    int h_err = 0;
-    TCA_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
-    TCA_CUDA_TRY(cudaStreamSynchronize(s));
-    if (h_err & kErrRowPtr)
-        return set_error(TCA_ERR_FORMAT, "row_ptr is not a valid CSR offset array (must start at 0, be non-decreasing and end at nnz=%d)", nnz);
-    if (h_err & kErrColRange)
-        return set_error(TCA_ERR_FORMAT, "a column index lies outside [0, K=%d)", K);
 
     // 2. row order
     k_iota<<<blocks_for(M, 256), 256, 0, s>>>(iota, M);
     if (p->opts.sort_rows) {
+        // row lengths are at most nnz: only their low bits take part
+        int end_bit = 1;
+        while (end_bit < 32 && ((long long)1 << end_bit) <= (long long)nnz) end_bit++;
         size_t tmp = 0;
-        TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, row_nnz, keys_out, iota, p->perm, M, 0, 32, s));
+        TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, row_nnz, keys_out, iota, p->perm, M, 0,
+                                                               end_bit, s));
         void *tbuf;
         TCA_TRY(dev_alloc((char **)&tbuf, tmp, nullptr)); t_cub.p = tbuf;
-        TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, row_nnz, keys_out, iota, p->perm, M, 0, 32, s));
+        TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, row_nnz, keys_out, iota, p->perm, M, 0,
+                                                               end_bit, s));
     } else {
         TCA_CUDA_TRY(cudaMemcpyAsync(p->perm, iota, sizeof(int) * M, cudaMemcpyDeviceToDevice, s));
     }
@@ -489,17 +497,17 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         char *tbuf;
         TCA_TRY(dev_alloc(&tbuf, tmp, nullptr)); tb.p = tbuf;
         TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tbuf, tmp, scan_in, p->p_row_ptr, M + 1, s));
-        TCA_CUDA_TRY(cudaStreamSynchronize(s)); // tb is freed at scope exit
-    }
-    k_permute<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(p->perm, row_ptr, col, val, p->p_row_ptr, M,
+    } // tb is released in stream order on s (DevBuf): no wait
+    if (vals_ready)
+        TCA_CUDA_TRY(cudaStreamWaitEvent(s, vals_ready, 0));
+    k_permute<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(p->perm, row_ptr, col, val, p->p_row_ptr, M, err,
                                                                  p->p_col, p->p_val, p->src);
     TCA_CUDA_TRY(cudaGetLastError());
-    // the sorted row offsets on the host (for the work items, step 7), read
-    // back with the window statistics under one synchronisation
-    std::vector<int> h_rp((size_t)M + 1);
-    TCA_CUDA_TRY(cudaMemcpyAsync(h_rp.data(), p->p_row_ptr, sizeof(int) * h_rp.size(), cudaMemcpyDeviceToHost, s));
 
-    // 3. windows
+    // 3. windows. The host reads, in one copy after one wait, everything it
+    // decides on: per window its distinct columns, nonzeros, sortedness and
+    // touched 64-column blocks, the check verdict and the sorted row offsets
+    // (for the work items, step 7), gathered in one device array.
     const int W = (M + kWindowRows - 1) / kWindowRows;
     p->n_windows = W;
     std::vector<int> h_all(W);
@@ -507,25 +515,33 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     TCA_TRY(dev_alloc(&p->all_windows, W, bytes));
     TCA_CUDA_TRY(cudaMemcpyAsync(p->all_windows, h_all.data(), sizeof(int) * W, cudaMemcpyHostToDevice, s));
 
-    std::vector<int> h_nu(W, 0), h_nnz(W, 0), h_elig(W, 0), h_nblk(W, 0);
+    const size_t n_stage = 4 * (size_t)W + 1 + (size_t)M + 1;
+    DevBuf t_stage;
+    int *d_stage;
+    TCA_TRY(dev_alloc(&d_stage, n_stage, nullptr)); t_stage.p = d_stage;
+    int *d_nu = d_stage, *d_wn = d_stage + W, *d_el = d_stage + 2 * W, *d_nb = d_stage + 3 * W;
     const bool tc_possible = (p->opts.path != 1) && K <= kMaxTcK && K > 0 && W > 0;
     if (tc_possible) {
-        DevBuf t_nu, t_wn, t_el, t_nb;
-        int *d_nu, *d_wn, *d_el, *d_nb;
-        TCA_TRY(dev_alloc(&d_nb, W, nullptr)); t_nb.p = d_nb;
-        TCA_TRY(dev_alloc(&d_nu, W, nullptr)); t_nu.p = d_nu;
-        TCA_TRY(dev_alloc(&d_wn, W, nullptr)); t_wn.p = d_wn;
-        TCA_TRY(dev_alloc(&d_el, W, nullptr)); t_el.p = d_el;
         const size_t smem = sizeof(uint32_t) * ((K + 31) / 32);
         TCA_CUDA_TRY(cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_window_stats<<<W, 1024, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, d_nu, d_wn, d_el, d_nb);
+        k_window_stats<<<W, 1024, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, err, d_nu, d_wn, d_el, d_nb);
         TCA_CUDA_TRY(cudaGetLastError());
-        TCA_CUDA_TRY(cudaMemcpyAsync(h_nu.data(), d_nu, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
-        TCA_CUDA_TRY(cudaMemcpyAsync(h_nnz.data(), d_wn, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
-        TCA_CUDA_TRY(cudaMemcpyAsync(h_elig.data(), d_el, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
-        TCA_CUDA_TRY(cudaMemcpyAsync(h_nblk.data(), d_nb, sizeof(int) * W, cudaMemcpyDeviceToHost, s));
+    } else if (W > 0) {
+        TCA_CUDA_TRY(cudaMemsetAsync(d_stage, 0, sizeof(int) * 4 * (size_t)W, s));
     }
+    TCA_CUDA_TRY(cudaMemcpyAsync(d_stage + 4 * W, err, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    TCA_CUDA_TRY(cudaMemcpyAsync(d_stage + 4 * W + 1, p->p_row_ptr, sizeof(int) * ((size_t)M + 1),
+                                 cudaMemcpyDeviceToDevice, s));
+    std::vector<int> h_stage(n_stage);
+    TCA_CUDA_TRY(cudaMemcpyAsync(h_stage.data(), d_stage, sizeof(int) * n_stage, cudaMemcpyDeviceToHost, s));
     TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    const int h_err = h_stage[4 * (size_t)W];
+    if (h_err & kErrRowPtr)
+        return set_error(TCA_ERR_FORMAT, "row_ptr is not a valid CSR offset array (must start at 0, be non-decreasing and end at nnz=%d)", nnz);
+    if (h_err & kErrColRange)
+        return set_error(TCA_ERR_FORMAT, "a column index lies outside [0, K=%d)", K);
+    const int *h_nu = h_stage.data(), *h_nnz = h_nu + W, *h_elig = h_nu + 2 * W, *h_nblk = h_nu + 3 * W;
+    const std::vector<int> h_rp(h_stage.begin() + 4 * (size_t)W + 1, h_stage.end());
 
     // 4. path decision (host, deterministic)
     // A window's chunks are "direct" (the 64-column blocks of K it touches,
@@ -647,7 +663,8 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     TCA_TRY(dev_alloc(&p->all_items, items.size(), bytes));
     if (!items.empty())
         TCA_CUDA_TRY(cudaMemcpyAsync(p->all_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
-    TCA_CUDA_TRY(cudaStreamSynchronize(s)); // the plan is complete, for work on any stream
+    if (sync_end)
+        TCA_CUDA_TRY(cudaStreamSynchronize(s)); // the plan is complete, for work on any stream
     return TCA_OK;
 }
 
@@ -707,21 +724,10 @@ int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alp
 }
 } // namespace tca
 
-using namespace tca;
-
-extern "C" {
-
-void tca_plan_opts_default(tca_plan_opts_t *o)
-{
-    if (!o) return;
-    *o = tca_plan_opts_t{};
-    o->sort_rows = 1;
-    o->tc_min_density = 0.02f;
-    o->path = 0;
-}
-
-int tca_plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16, int M, int K, int nnz,
-                    const tca_plan_opts_t *opts, tca_stream_t stream, tca_plan_t *plan)
+namespace tca {
+int plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16, int M, int K, int nnz,
+                const tca_plan_opts_t *opts, cudaStream_t stream, cudaEvent_t vals_ready, bool sync_end,
+                tca_plan_t *plan)
 {
     clear_error();
     if (!plan)
@@ -742,13 +748,33 @@ int tca_plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_va
     p->M = M; p->K = K; p->nnz = nnz; p->opts = o;
     int st = TCA_OK;
     if (M > 0)
-        st = build_plan(p, d_row_ptr, d_col_idx, (const __half *)d_vals_f16, (cudaStream_t)stream);
+        st = build_plan(p, d_row_ptr, d_col_idx, (const __half *)d_vals_f16, stream, vals_ready, sync_end);
     if (st != TCA_OK) {
         free_plan(p);
         return st;
     }
     *plan = p;
     return TCA_OK;
+}
+} // namespace tca
+
+using namespace tca;
+
+extern "C" {
+
+void tca_plan_opts_default(tca_plan_opts_t *o)
+{
+    if (!o) return;
+    *o = tca_plan_opts_t{};
+    o->sort_rows = 1;
+    o->tc_min_density = 0.02f;
+    o->path = 0;
+}
+
+int tca_plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16, int M, int K, int nnz,
+                    const tca_plan_opts_t *opts, tca_stream_t stream, tca_plan_t *plan)
+{
+    return plan_create(d_row_ptr, d_col_idx, d_vals_f16, M, K, nnz, opts, (cudaStream_t)stream, nullptr, true, plan);
 }
 
 int tca_plan_update_values(tca_plan_t p, const void *d_vals_f16, tca_stream_t stream)

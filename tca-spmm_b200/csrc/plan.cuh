@@ -184,6 +184,13 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
 int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
                          cudaStream_t s, void *const *events, bool no_alloc = false);
 
+// tca_plan_create with two extra controls for the host-buffer forward:
+// vals_ready (an event after which the values may be read; NULL: at once)
+// and sync_end (false: the build is only ordered on `stream`, not waited for).
+int plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16, int M, int K, int nnz,
+                const tca_plan_opts_t *opts, cudaStream_t stream, cudaEvent_t vals_ready, bool sync_end,
+                tca_plan_t *plan);
+
 // The N-slice width a single forward of this plan uses (split: the launch
 // cuts items by chunk ranges).
 int pick_tc_tile(const tca_plan *p, int N, bool batched, bool f8 = false, bool split = true);
