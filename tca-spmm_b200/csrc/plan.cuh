@@ -139,25 +139,25 @@ struct SpmmJob {
 using LaunchList = std::vector<std::function<int(cudaStream_t)>>;
 
 // Device workspace of the tensor-core launches of one call whose work is
-// split across CTAs by chunk ranges: the arrival counters (zero before the
-// first launch; the launches leave them zero) and the partial tiles. The
-// caller allocates partial_bytes (as reported by launch_tc_jobs) before
-// running the deferred launches.
+// split across CTAs by chunk ranges: the partial tiles of cut items, one
+// region per launch, and a word that a CTA which gave up sets. The caller allocates partial_bytes (as reported by
+// launch_tc_jobs) before running the deferred launches.
 struct TcWorkspace {
     size_t partial_bytes = 0;
     float *partials = nullptr;
-    int *arrivals = nullptr;
+    int *failed = nullptr; // cleared before the launches
 };
-constexpr int kArrivalSlots = 2 * kSMs;
 
 // Tensor-core (tcgen05) forward over the tensor-core windows of every job
 // (jobs with tc set), in as few launches as the N-slice widths allow. With
 // `defer` the prepared launches are appended to it instead of issued. With a
-// workspace, launches split their work across CTAs by chunk ranges where
-// that fits (and record the partial-tile bytes they need in it); without,
+// workspace (and `post`), launches split their work across CTAs by chunk
+// ranges where that fits, record the partial-tile bytes they need in it, and
+// append to `post` the launches that add up the cut items' parts -- to be
+// issued after every launch of `defer` and of the CUDA-core list; without,
 // every item runs whole on one CTA (nothing to allocate).
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s, LaunchList *defer, TcWorkspace *ws);
+                   cudaStream_t s, LaunchList *defer, TcWorkspace *ws, LaunchList *post);
 
 // Registers that one block of the tensor-core kernel holds on an SM (the
 // largest over its FP16 or its E4M3 instantiations).

@@ -24,11 +24,12 @@
 //
 // When the windows' groups are fewer than the SMs, the n range is cut into
 // parts; each part leaves its values in a workspace slice (one float per
-// tensor-core entry) and the part that arrives last (arrival counter per
-// group) adds the parts in part order -- a fixed order, so the result does not
-// depend on which part finishes last -- and writes dA. No CTA waits for
-// another. Every mbarrier wait is bounded (about one second); on expiry the
-// CTA records kStatusTimeout in the plan's status word and ends.
+// tensor-core entry), and after the launch k_sddmm_sum adds the parts of
+// every entry in part order -- a fixed order, so the result does not depend
+// on which part finished when -- and writes dA. No CTA waits for another.
+// Every mbarrier wait is bounded (about one second); on expiry the CTA records
+// kStatusTimeout in the plan's status word (and in the launch's failure word,
+// so that the sums are skipped) and ends.
 #include <cuda.h>
 #include <algorithm>
 #include "tca_internal.cuh"
@@ -69,7 +70,7 @@ struct SdJob {
     const uint32_t *entries;
     void *out;             // nnz values in the caller's order (FP16 or FP32)
     float *partials;       // parts > 1: parts x tc_nnz floats
-    int *arrivals;         // parts > 1: one counter per group, zero between launches
+    int *failed;           // parts > 1: set when a CTA gave up (zero before the launch)
     int *status;
     int M, N, n_steps, parts, steps_per_part, out_f16;
     int n_win, groups_per_win; // tensor-core windows; chunk groups of the widest window
@@ -120,7 +121,6 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
     uint64_t *acc_full = b_empty + kSdBStages;
     uint64_t *drain = acc_full + 1;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
-    volatile int *last_flag = reinterpret_cast<volatile int *>(drain + 1) + 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     SdUnit x;
@@ -262,7 +262,6 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
             // the MMAs are complete, so the dY ring is free: it holds the
             // staging tile (row-major, kSdStageRow floats a row)
             float *stage = reinterpret_cast<float *>(smem + kSdYOff);
-            const int e_lo = __ldg(a.tile_ptr + c_first), e_hi = __ldg(a.tile_ptr + c_first + x.nch);
             for (int c = 0; c < x.nch; c++) {
 #pragma unroll
                 for (int cb = 0; cb < 4; cb++) {
@@ -291,31 +290,6 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
                 }
                 named_bar_sync(1, kSdEpiThreads); // the staging tile is reused by the next chunk
             }
-            if (a.parts > 1) {
-                __threadfence();
-                named_bar_sync(1, kSdEpiThreads);
-                if (et == 0) {
-                    const int last = atomicAdd(a.arrivals + x.group, 1) == a.parts - 1;
-                    if (last) {
-                        a.arrivals[x.group] = 0; // every part has arrived: ready for the next launch
-                        __threadfence();
-                    }
-                    *last_flag = last;
-                }
-                named_bar_sync(1, kSdEpiThreads);
-                if (*last_flag) {
-                    __threadfence();
-                    for (int e = e_lo + et; e < e_hi; e += kSdEpiThreads) {
-                        float d = __ldcg(a.partials + e);
-                        for (int q = 1; q < a.parts; q++) d += __ldcg(a.partials + (size_t)q * a.tc_nnz + e);
-                        const int j = __ldg(a.src + __ldg(a.tile_src + e));
-                        if (a.out_f16)
-                            reinterpret_cast<__half *>(a.out)[j] = __float2half_rn(a.alpha * d);
-                        else
-                            reinterpret_cast<float *>(a.out)[j] = a.alpha * d;
-                    }
-                }
-            }
         }
     }
 
@@ -326,6 +300,8 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
         // shared memory is released
         if (threadIdx.x == 0) {
             atomicOr(a.status, kStatusTimeout);
+            if (a.failed)
+                atomicOr(a.failed, 1);
             const uint64_t t0 = global_ns();
             while (global_ns() - t0 < 1000000ull) {
             }
@@ -335,6 +311,38 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
     if (warp == kSdMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tcols) : "memory");
+    }
+}
+
+// After a launch with parts: dA of every tensor-core entry e = alpha x (part
+// 0 + part 1 + ...) in part order, written in the caller's nonzero order;
+// nothing when a CTA of the launch gave up.
+template <typename OutT>
+__global__ void __launch_bounds__(256)
+k_sddmm_sum(const float *__restrict__ partials, long long tc_nnz, int parts, const int *__restrict__ tile_src,
+            const int *__restrict__ src, const int *__restrict__ failed, OutT *__restrict__ out, float alpha)
+{
+    if (*(volatile const int *)failed)
+        return;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tc_nnz;
+         e += (long long)gridDim.x * blockDim.x) {
+        float x[8];
+        float d = 0.f;
+        for (int q0 = 0; q0 < parts; q0 += 8) {
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (q0 + u < parts)
+                    x[u] = __ldcg(partials + (size_t)(q0 + u) * tc_nnz + e);
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (q0 + u < parts)
+                    d = (q0 + u == 0) ? x[u] : d + x[u];
+        }
+        const int j = __ldg(src + __ldg(tile_src + e));
+        if constexpr (sizeof(OutT) == 2)
+            out[j] = __float2half_rn(alpha * d);
+        else
+            out[j] = alpha * d;
     }
 }
 
@@ -386,28 +394,37 @@ int sddmm_tc(const tca_plan *p, const __half *dY, int ldy, const __half *B, int 
     j.n_win = p->n_tc;
     j.groups_per_win = groups_per_win;
 
-    // with parts: arrival counters (cleared) and partial values, for this
-    // call only (stream-ordered; under capture the graph's own memory)
+    // with parts: the failure word (cleared) and the partial values, for
+    // this call only (stream-ordered; under capture the graph's own memory)
     void *ws = nullptr;
-    const size_t cnt = ((sizeof(int) * (size_t)n_groups) + 255) & ~(size_t)255;
     if (parts > 1) {
         cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
         TCA_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
-        const size_t bytes = cnt + sizeof(float) * (size_t)parts * (size_t)p->tc_nnz;
+        const size_t bytes = 256 + sizeof(float) * (size_t)parts * (size_t)p->tc_nnz;
         if (cap == cudaStreamCaptureStatusActive)
             TCA_CUDA_TRY(cudaMallocAsync(&ws, bytes, s));
         else
             TCA_TRY(dev_malloc(&ws, bytes, s));
-        j.arrivals = static_cast<int *>(ws);
-        j.partials = reinterpret_cast<float *>(static_cast<char *>(ws) + cnt);
+        j.failed = static_cast<int *>(ws);
+        j.partials = reinterpret_cast<float *>(static_cast<char *>(ws) + 256);
     }
     cudaError_t e = cudaSuccess;
     if (ws)
-        e = cudaMemsetAsync(j.arrivals, 0, sizeof(int) * (size_t)n_groups, s);
+        e = cudaMemsetAsync(j.failed, 0, sizeof(int), s);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_sddmm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSdSmem);
     if (e == cudaSuccess) {
         k_sddmm_tc<<<n_groups * parts, kSdThreads, kSdSmem, s>>>(j);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && ws) {
+        const unsigned grid = (unsigned)std::min<long long>((p->tc_nnz + 255) / 256, 8LL * kSMs);
+        if (out_f16)
+            k_sddmm_sum<__half><<<grid, 256, 0, s>>>(j.partials, p->tc_nnz, parts, p->tile_src, p->src, j.failed,
+                                                      static_cast<__half *>(out), alpha);
+        else
+            k_sddmm_sum<float><<<grid, 256, 0, s>>>(j.partials, p->tc_nnz, parts, p->tile_src, p->src, j.failed,
+                                                     static_cast<float *>(out), alpha);
         e = cudaGetLastError();
     }
     if (ws)

@@ -89,20 +89,26 @@ struct TcJob {
 // Chunk ranges (stream-K): the items' chunks, job by job, window by window,
 // N slice by N slice, are `units` chunk-units; CTA b covers units
 // [b * units / grid, (b + 1) * units / grid), starting in item
-// cta_start[b] = {job, window, N slice, chunk within the item}. Cut items
-// leave partial tiles in `partials` (two slots of 128 x NT floats per CTA:
-// slot 2b for the CTA's first segment when that is cut, 2b + 1 for its last)
-// and count arrivals in `arrivals` (one per slot; every counter is zero
-// between launches: the last arriver resets it).
+// cta_start[b] = {job, window, N slice, chunk within the item}. A cut item's
+// parts leave partial tiles in `partials` (two slots of 128 x NT floats per
+// CTA: slot 2b for the CTA's first segment when that is cut, 2b + 1 for its
+// last; tc_slot), which spmm_tc_fixup adds up after the launch.
 struct TcBatch {
     int n_jobs;
     int item_start[kMaxJobs + 1];
     int split;        // 1: chunk ranges (above); 0: item i to CTA i mod grid
     long long units;
     float *partials;
-    int *arrivals;
+    int *failed;      // split launches: set when a CTA gave up (zero before the launch); the sums are then skipped
     int4 cta_start[kSMs];
     TcJob job[kMaxJobs];
+};
+
+// The cut items of a split launch: {job << 16 | N slice, tensor-core window,
+// first CTA, parts << 1 | head}, head: part 0 is its CTA's first segment.
+struct TcCuts {
+    int n;
+    int4 cut[kSMs];
 };
 
 // The CTA whose range holds chunk-unit u (ranges of units / grid, floored).
@@ -169,6 +175,28 @@ __device__ __forceinline__ void store8_out(float *p, const float *v, float alpha
     }
     reinterpret_cast<float4 *>(p)[0] = make_float4(o[0], o[1], o[2], o[3]);
     reinterpret_cast<float4 *>(p)[1] = make_float4(o[4], o[5], o[6], o[7]);
+}
+
+// Slot of part q of a cut item whose first part is on CTA b0 (head: that part
+// is CTA b0's first segment): part q > 0 is the first segment of CTA b0 + q.
+__host__ __device__ inline int tc_slot(int b0, int q, bool head)
+{
+    return q > 0 ? 2 * (b0 + q) : 2 * b0 + (head ? 0 : 1);
+}
+
+// E4M3 dequantisation of 16 accumulators of columns n..n+15: row scale x
+// column scale (16-byte aligned scale vectors; columns >= N read as 0).
+__device__ __forceinline__ void dequant16(float *v, float sa, const float *col_scale, int n, int N)
+{
+    const float4 *cs = reinterpret_cast<const float4 *>(col_scale + n);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const float4 sv = (n + 4 * q < N) ? __ldg(cs + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        v[4 * q] *= sa * sv.x;
+        v[4 * q + 1] *= sa * sv.y;
+        v[4 * q + 2] *= sa * sv.z;
+        v[4 * q + 3] *= sa * sv.w;
+    }
 }
 
 // Shared memory (1024-byte aligned base): kStages x (A tile | B tile),
@@ -262,7 +290,6 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     volatile int *flag = reinterpret_cast<volatile int *>(drain + 1); // 2 slots per scatter group
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1) + 4;
     volatile int *seg_count = reinterpret_cast<volatile int *>(drain + 1) + 5;
-    volatile int *epi_last = reinterpret_cast<volatile int *>(drain + 1) + 6;
     constexpr int kScatterGroups = S % 2 == 0 ? 2 : 1; // two groups need an even ring (see the scatter role)
     constexpr int kGroupThreads = kScatterThreads / kScatterGroups;
 
@@ -328,6 +355,20 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                 if (w >= a.n_win) { j++; w = 0; }
             }
             if (lane == 0) {
+                // The range's last segment, when cut, is the head of an item
+                // another CTA finishes: it goes second (after the first,
+                // itself cut or whole), so that both cut parts complete early
+                // and the part that adds them up does so while this CTA's
+                // whole items still run.
+                if (n >= 3 && parts[n - 1].z > 1) {
+                    const int4 li = items[n - 1], lp = parts[n - 1];
+                    for (int k = n - 1; k > 1; k--) {
+                        items[k] = items[k - 1];
+                        parts[k] = parts[k - 1];
+                    }
+                    items[1] = li;
+                    parts[1] = lp;
+                }
                 *seg_count = n;
                 if (u < hi) // more segments than the table holds: the host sizes ranges so that this cannot be
                     atomicOr(batch.job[0].status, kStatusTable);
@@ -530,15 +571,11 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     } else {
         // ---------------- epilogue ----------------
         // Per segment: wait for its accumulator; a whole item is stored to C
-        // (alpha, beta, E4M3 scales). A cut item's part leaves its FP32
-        // partial tile in its slot; the part that arrives last (arrival
-        // counter) adds all parts in part order -- its own from tensor memory
-        // -- and stores C.
+        // (alpha, beta, E4M3 scales); a cut item's part leaves its FP32
+        // partial tile in its slot, for spmm_tc_fixup to add up after this
+        // launch.
         const int quarter = warp & 3;
         const int row = quarter * 32 + lane; // TMEM lane = row of the window
-        auto slot_of = [&](const int4 &pt, int q) {
-            return q > 0 ? 2 * (pt.x + q) : 2 * pt.x + (pt.w ? 0 : 1);
-        };
         for (int k = 0; k < n_items; k++) {
             const int4 it = items[k];
             const int4 pt = parts[k];
@@ -557,9 +594,8 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             if (!named_bar_and(kEpiBar, kEpiThreads, got != 0)) { ok = false; break; }
             tc_fence_after();
             const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * NT);
-            bool store = true;
             if (pt.z > 1) {
-                float *mine = batch.partials + ((size_t)slot_of(pt, pt.y) * kWindowRows + row) * NT;
+                float *mine = batch.partials + ((size_t)tc_slot(pt.x, pt.y, pt.w != 0) * kWindowRows + row) * NT;
                 for (int cb = 0; cb < NT / 16; cb++) {
                     if (n0 + cb * 16 >= a.N)
                         break; // uniform across the warp
@@ -571,72 +607,25 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
                         dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
                                              __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
                 }
-                __threadfence();
-                named_bar_sync(kEpiBar, kEpiThreads);
-                if (warp == kMmaWarp + 1 && lane == 0) {
-                    const int key = slot_of(pt, 0);
-                    const int last = atomicAdd(batch.arrivals + key, 1) == pt.z - 1;
-                    if (last) {
-                        batch.arrivals[key] = 0; // every part has arrived: ready for the next launch
-                        __threadfence();
+            } else {
+                OutT *Crow = out_row >= 0 ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
+                float sa = 1.f;
+                if constexpr (F8)
+                    sa = (i < a.M) ? a.row_scale[i] : 0.f;
+                for (int cb = 0; cb < NT / 16; cb++) {
+                    const int n = n0 + cb * 16;
+                    if (n >= a.N)
+                        break; // uniform across the warp
+                    uint32_t r[16];
+                    tmem_ld16(taddr + cb * 16, r);
+                    float *v = reinterpret_cast<float *>(r);
+                    if constexpr (F8)
+                        dequant16(v, sa, a.col_scale, n, a.N);
+                    if (Crow) {
+                        store8_out(Crow + n, v, a.alpha, a.beta);
+                        if (n + 8 < a.N)
+                            store8_out(Crow + n + 8, v + 8, a.alpha, a.beta);
                     }
-                    *epi_last = last;
-                }
-                named_bar_sync(kEpiBar, kEpiThreads);
-                store = *epi_last != 0;
-                if (store)
-                    __threadfence();
-            }
-            OutT *Crow = (store && out_row >= 0) ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
-            float sa = 1.f;
-            if constexpr (F8)
-                sa = (i < a.M) ? a.row_scale[i] : 0.f;
-            for (int cb = 0; store && cb < NT / 16; cb++) {
-                const int n = n0 + cb * 16;
-                if (n >= a.N)
-                    break; // uniform across the warp
-                uint32_t r[16];
-                tmem_ld16(taddr + cb * 16, r);
-                float *f = reinterpret_cast<float *>(r);
-                if (pt.z > 1) { // the parts in order: part q from its slot, this CTA's own from tensor memory
-                    float v[16];
-                    for (int q = 0; q < pt.z; q++) {
-                        if (q == pt.y) {
-#pragma unroll
-                            for (int e = 0; e < 16; e++) v[e] = q == 0 ? f[e] : v[e] + f[e];
-                        } else {
-                            const float4 *srcp = reinterpret_cast<const float4 *>(
-                                batch.partials + ((size_t)slot_of(pt, q) * kWindowRows + row) * NT + cb * 16);
-#pragma unroll
-                            for (int e4 = 0; e4 < 4; e4++) {
-                                const float4 x = __ldcg(srcp + e4);
-                                const float xs[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-                                for (int e = 0; e < 4; e++) v[4 * e4 + e] = q == 0 ? xs[e] : v[4 * e4 + e] + xs[e];
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int e = 0; e < 16; e++) f[e] = v[e];
-                }
-                if constexpr (F8) { // dequantise: row scale x column scale (16-byte aligned scale vectors)
-                    const float4 *cs = reinterpret_cast<const float4 *>(a.col_scale + n);
-                    float sb[16];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const float4 v = (n + 4 * q < a.N) ? __ldg(cs + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-                        sb[4 * q] = v.x;
-                        sb[4 * q + 1] = v.y;
-                        sb[4 * q + 2] = v.z;
-                        sb[4 * q + 3] = v.w;
-                    }
-#pragma unroll
-                    for (int q = 0; q < 16; q++) f[q] *= sa * sb[q];
-                }
-                if (Crow) {
-                    store8_out(Crow + n, f, a.alpha, a.beta);
-                    if (n + 8 < a.N)
-                        store8_out(Crow + n + 8, f + 8, a.alpha, a.beta);
                 }
             }
             tc_fence_before();
@@ -653,6 +642,8 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         if (threadIdx.x == 0) {
             if (n_items > 0)
                 atomicOr(batch.job[items[0].w >> 16].status, kStatusTimeout);
+            if (batch.split)
+                atomicOr(batch.failed, 1); // its cut parts may be missing: no sums after this launch
             const uint64_t t0 = global_ns();
             while (global_ns() - t0 < 1000000ull) {
             }
@@ -662,6 +653,68 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * NT) : "memory");
+    }
+}
+
+// After a split launch: block (c, r) adds up the parts of cut item c for
+// rows 32 r .. 32 r + 31 of its window, in part order -- a fixed order, so the
+// result does not depend on which CTA computed which part when -- and stores
+// C as the tensor-core epilogue stores a whole item (E4M3 scales, alpha,
+// beta, rows without nonzeros kept on request). A thread takes 8 columns of a
+// row; the loads of up to four parts are issued before the first is added.
+template <int NT, typename OutT, bool F8>
+__global__ void __launch_bounds__(256)
+spmm_tc_fixup(const __grid_constant__ TcBatch batch, const __grid_constant__ TcCuts cuts)
+{
+    if (*(volatile const int *)batch.failed)
+        return; // a CTA of the launch gave up (its status word says so): C keeps what it had
+    const int4 cu = cuts.cut[blockIdx.x];
+    const TcJob &a = batch.job[cu.x >> 16];
+    const int n0 = (cu.x & 0xffff) * NT;
+    const int window = __ldg(&a.win_info[cu.y].x);
+    const int b0 = cu.z, parts = cu.w >> 1;
+    const bool head = (cu.w & 1) != 0;
+    const int vpr = min(NT, a.N - n0) >> 3; // 8-column vectors a row (N % 8 == 0 on this path)
+    for (int idx = threadIdx.x; idx < 32 * vpr; idx += blockDim.x) {
+        const int rl = blockIdx.y * 32 + idx / vpr, c8 = (idx % vpr) * 8;
+        const int i = window * kWindowRows + rl;
+        if (i >= a.M)
+            continue;
+        const size_t off = (size_t)rl * NT + c8;
+        float acc[8];
+        for (int q0 = 0; q0 < parts; q0 += 4) {
+            float4 x[4][2];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (q0 + u < parts) {
+                    const float4 *src = reinterpret_cast<const float4 *>(
+                        batch.partials + (size_t)tc_slot(b0, q0 + u, head) * kWindowRows * NT + off);
+                    x[u][0] = __ldcg(src);
+                    x[u][1] = __ldcg(src + 1);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if (q0 + u < parts) {
+                    const float e[8] = {x[u][0].x, x[u][0].y, x[u][0].z, x[u][0].w,
+                                        x[u][1].x, x[u][1].y, x[u][1].z, x[u][1].w};
+#pragma unroll
+                    for (int k = 0; k < 8; k++) acc[k] = (q0 + u == 0) ? e[k] : acc[k] + e[k];
+                }
+            }
+        }
+        if ((a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) && a.p_row_ptr[i + 1] == a.p_row_ptr[i])
+            continue;
+        const int n = n0 + c8;
+        if constexpr (F8) {
+            const float sa = a.row_scale[i];
+            const float4 s0 = __ldg(reinterpret_cast<const float4 *>(a.col_scale + n));
+            const float4 s1 = __ldg(reinterpret_cast<const float4 *>(a.col_scale + n) + 1);
+            const float sb[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+#pragma unroll
+            for (int k = 0; k < 8; k++) acc[k] *= sa * sb[k];
+        }
+        store8_out(reinterpret_cast<OutT *>(a.C) + (size_t)a.perm[i] * a.ldc + n, acc, a.alpha, a.beta);
     }
 }
 
@@ -759,10 +812,11 @@ int make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT,
 // has few parts to add up) and each CTA's start item, from the plans' host
 // copies of their windows' chunk offsets. False when some CTA's range would
 // reach more items than its work table holds (then items go to CTAs in turn).
-constexpr int kMinUnits = 4;
+constexpr int kMinUnits = 8;
 
-bool plan_ranges(TcBatch &b, const tca_plan *const *plans, int *grid_out)
+bool plan_ranges(TcBatch &b, const tca_plan *const *plans, int *grid_out, TcCuts *cuts)
 {
+    cuts->n = 0;
     long long units = 0;
     for (int j = 0; j < b.n_jobs; j++)
         units += (long long)plans[j]->n_tc_chunks * b.job[j].ntiles;
@@ -777,6 +831,12 @@ bool plan_ranges(TcBatch &b, const tca_plan *const *plans, int *grid_out)
             const int z = first[w + 1] - first[w];
             for (int t = 0; t < b.job[j].ntiles; t++, u0 += z) {
                 const int c0 = range_owner(u0, units, G), c1 = range_owner(u0 + z - 1, units, G);
+                if (c1 > c0) {
+                    if (cuts->n == kSMs)
+                        return false; // cannot happen: a cut needs a range boundary inside the item
+                    const int head = range_lo(c0, units, G) == u0 ? 1 : 0;
+                    cuts->cut[cuts->n++] = make_int4((j << 16) | t, w, c0, ((c1 - c0 + 1) << 1) | head);
+                }
                 for (int c = c0; c <= c1; c++) {
                     if (++segs[c] > kMaxCtaItems)
                         return false;
@@ -801,6 +861,26 @@ int launch_group(const TcBatch &b, int grid, cudaStream_t s)
     spmm_tc_kernel<NT, OutT, F8><<<grid, kThreads, smem, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
+}
+
+template <int NT, typename OutT, bool F8>
+int launch_fixup(const TcBatch &b, const TcCuts &c, cudaStream_t s)
+{
+    spmm_tc_fixup<NT, OutT, F8><<<dim3((unsigned)c.n, kWindowRows / 32), 256, 0, s>>>(b, c);
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
+template <typename OutT>
+int launch_fixup_out(const TcBatch &b, const TcCuts &c, int NT, bool f8, cudaStream_t s)
+{
+    if (f8)
+        return NT == 128 ? launch_fixup<128, OutT, true>(b, c, s) : launch_fixup<256, OutT, true>(b, c, s);
+    switch (NT) {
+    case 64: return launch_fixup<64, OutT, false>(b, c, s);
+    case 128: return launch_fixup<128, OutT, false>(b, c, s);
+    default: return launch_fixup<256, OutT, false>(b, c, s);
+    }
 }
 
 template <typename OutT>
@@ -880,7 +960,7 @@ int tc_block_regs(bool f8, int *regs)
 }
 
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s, LaunchList *defer, TcWorkspace *ws)
+                   cudaStream_t s, LaunchList *defer, TcWorkspace *ws, LaunchList *post)
 {
     const int widths[3] = {64, 128, 256};
     auto emit = [&](TcBatch &b, const tca_plan *const *plans, int NT, bool f8) -> int {
@@ -891,20 +971,30 @@ int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
         b.split = 0;
         b.units = 0;
         b.partials = nullptr;
-        b.arrivals = nullptr;
-        if (ws && plan_ranges(b, plans, &grid))
-            ws->partial_bytes = std::max(ws->partial_bytes, sizeof(float) * 2 * (size_t)grid * kWindowRows * NT);
+        b.failed = nullptr;
+        auto cuts = std::make_shared<TcCuts>();
+        cuts->n = 0;
+        size_t offset = 0; // this launch's partial tiles in the workspace (floats)
+        if (ws && defer && post && plan_ranges(b, plans, &grid, cuts.get())) {
+            offset = ws->partial_bytes / sizeof(float);
+            // every launch of the call has a region of its own: the fixups run after all of them
+            ws->partial_bytes += sizeof(float) * 2 * (size_t)grid * kWindowRows * NT;
+        }
         if (!defer)
-            return b.split ? set_error(TCA_ERR_INVALID_ARG, "a split launch needs its workspace")
-                           : launch_group_typed(b, NT, f8, c_dtype, grid, s);
+            return launch_group_typed(b, NT, f8, c_dtype, grid, s);
         auto held = std::make_shared<TcBatch>(b);
-        defer->push_back([held, NT, f8, c_dtype, grid, ws](cudaStream_t st) {
+        defer->push_back([held, NT, f8, c_dtype, grid, ws, offset](cudaStream_t st) {
             if (held->split) {
-                held->partials = ws->partials;
-                held->arrivals = ws->arrivals;
+                held->partials = ws->partials + offset;
+                held->failed = ws->failed;
             }
             return launch_group_typed(*held, NT, f8, c_dtype, grid, st);
         });
+        if (held->split && cuts->n > 0)
+            post->push_back([held, cuts, NT, f8, c_dtype](cudaStream_t st) {
+                return c_dtype == TCA_DTYPE_F16 ? launch_fixup_out<__half>(*held, *cuts, NT, f8, st)
+                                                : launch_fixup_out<float>(*held, *cuts, NT, f8, st);
+            });
         return TCA_OK;
     };
     for (bool f8 : {false, true}) {
