@@ -664,12 +664,11 @@ int tca_spmm_fp8_static(tca_plan_t p, const void *d_B_f16, int ldb, int N, void 
     job.ldc = ldc;
     job.f8 = true;
     job.tc = p->n_tc > 0;
-    job.n_tile = pick_tc_tile(p, N, false, true, false);
+    job.n_tile = pick_tc_tile(p, N, false, true);
     job.Bq = Bq;
     job.ldq = ldq;
     job.col_scale = scale;
     // the launches of tca_spmm_fp8 (the CUDA-core launch runs beside the
-    // tensor-core launch as its programmatic dependent), with every item run
-    // whole on one CTA: nothing to allocate for split items
-    return run_jobs_with_events(&job, 1, c_dtype, alpha, beta, flags, s, nullptr, true);
+    // tensor-core launch as its programmatic dependent); they allocate nothing
+    return run_jobs_with_events(&job, 1, c_dtype, alpha, beta, flags, s, nullptr);
 }

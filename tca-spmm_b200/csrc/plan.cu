@@ -673,14 +673,13 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
 
 namespace tca {
 int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                         cudaStream_t s, void *const *events, bool no_alloc)
+                         cudaStream_t s, void *const *events)
 {
     // Without events the CUDA-core launches follow the tensor-core launch as
     // programmatic dependents and run beside it; with events (which time each
     // path alone) the two run one after the other.
-    LaunchList tc, cc, post;
-    TcWorkspace ws;
-    TCA_TRY(launch_tc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &tc, no_alloc ? nullptr : &ws, &post));
+    LaunchList tc, cc;
+    TCA_TRY(launch_tc_jobs(jobs, n_jobs, c_dtype, alpha, beta, flags, s, &tc));
     int beside = 0;
     for (int i = 0; !events && !tc.empty() && i < n_jobs; i++) {
         int r = 0;
@@ -691,39 +690,20 @@ int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alp
     // Under stream capture a plain record only orders the graph; an external
     // record becomes a graph node that records the event at every replay.
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    TCA_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
-    const bool capturing = cap == cudaStreamCaptureStatusActive;
-    // the split launches' partial tiles, for this call only (stream-ordered:
-    // under capture the graph's own memory, otherwise the library's pool)
-    void *wsp = nullptr;
-    if (ws.partial_bytes > 0) {
-        if (capturing)
-            TCA_CUDA_TRY(cudaMallocAsync(&wsp, 256 + ws.partial_bytes, s));
-        else
-            TCA_TRY(dev_malloc(&wsp, 256 + ws.partial_bytes, s));
-        ws.failed = static_cast<int *>(wsp);
-        ws.partials = reinterpret_cast<float *>(static_cast<char *>(wsp) + 256);
-        TCA_CUDA_TRY(cudaMemsetAsync(ws.failed, 0, sizeof(int), s));
-    }
-    const unsigned rec_flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    if (events)
+        TCA_CUDA_TRY(cudaStreamIsCapturing(s, &cap));
+    const unsigned rec_flags = cap == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
     auto rec = [&](int i) -> int {
         if (events && events[i]) TCA_CUDA_TRY(cudaEventRecordWithFlags((cudaEvent_t)events[i], s, rec_flags));
         return TCA_OK;
     };
-    // with events the cut items' sums belong to the tensor-core time: they
-    // follow the tensor-core launches; without, the CUDA-core launches come
-    // first (beside the tensor-core launch) and the sums after them
-    int st = rec(0);
-    for (size_t i = 0; st == TCA_OK && i < tc.size(); i++) st = tc[i](s);
-    for (size_t i = 0; events && st == TCA_OK && i < post.size(); i++) st = post[i](s);
-    if (st == TCA_OK) st = rec(1);
-    if (st == TCA_OK) st = rec(2);
-    for (size_t i = 0; st == TCA_OK && i < cc.size(); i++) st = cc[i](s);
-    if (st == TCA_OK) st = rec(3);
-    for (size_t i = 0; !events && st == TCA_OK && i < post.size(); i++) st = post[i](s);
-    if (wsp)
-        cudaFreeAsync(wsp, s); // after every launch of the call in stream order
-    return st;
+    TCA_TRY(rec(0));
+    for (auto &f : tc) TCA_TRY(f(s));
+    TCA_TRY(rec(1));
+    TCA_TRY(rec(2));
+    for (auto &f : cc) TCA_TRY(f(s));
+    TCA_TRY(rec(3));
+    return TCA_OK;
 }
 } // namespace tca
 

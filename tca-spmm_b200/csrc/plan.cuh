@@ -60,7 +60,7 @@ struct tca_plan {
     int2 *all_items = nullptr;
     int n_cc_items = 0, n_all_items = 0;
     // host copy of tile_first: chunk offsets of the tensor-core windows
-    // (n_tc + 1), for sizing the launches' chunk ranges
+    // (n_tc + 1), for sizing launches on the host
     std::vector<int> h_tile_first;
     int *d_status = nullptr; // device error word written by bounded waits
     size_t bytes = 0;
@@ -115,7 +115,6 @@ constexpr int kMaxTcK = 1 << 17;
 // Device status bits.
 constexpr int kStatusTimeout = 1;
 constexpr int kStatusLayout = 2; // shared memory base not 1024-byte aligned: the kernel did no work
-constexpr int kStatusTable = 4;  // a CTA's chunk range held more items than its work table: work was left out
 
 // One forward of one plan, as the batched launchers see it.
 struct SpmmJob {
@@ -138,26 +137,11 @@ struct SpmmJob {
 // descriptors) is already done: running one only launches.
 using LaunchList = std::vector<std::function<int(cudaStream_t)>>;
 
-// Device workspace of the tensor-core launches of one call whose work is
-// split across CTAs by chunk ranges: the partial tiles of cut items, one
-// region per launch, and a word that a CTA which gave up sets. The caller allocates partial_bytes (as reported by
-// launch_tc_jobs) before running the deferred launches.
-struct TcWorkspace {
-    size_t partial_bytes = 0;
-    float *partials = nullptr;
-    int *failed = nullptr; // cleared before the launches
-};
-
 // Tensor-core (tcgen05) forward over the tensor-core windows of every job
 // (jobs with tc set), in as few launches as the N-slice widths allow. With
-// `defer` the prepared launches are appended to it instead of issued. With a
-// workspace (and `post`), launches split their work across CTAs by chunk
-// ranges where that fits, record the partial-tile bytes they need in it, and
-// append to `post` the launches that add up the cut items' parts -- to be
-// issued after every launch of `defer` and of the CUDA-core list; without,
-// every item runs whole on one CTA (nothing to allocate).
+// `defer` the prepared launches are appended to it instead of issued.
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s, LaunchList *defer, TcWorkspace *ws, LaunchList *post);
+                   cudaStream_t s, LaunchList *defer = nullptr);
 
 // Registers that one block of the tensor-core kernel holds on an SM (the
 // largest over its FP16 or its E4M3 instantiations).
@@ -177,12 +161,9 @@ int launch_cc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
 // CUDA-core launches, so that the events bracket device work only. Without
 // events, the CUDA-core launches run concurrently with the tensor-core launch
 // (programmatic dependents on the same stream; the two paths write disjoint
-// rows of C). The tensor-core work is split across CTAs by chunk ranges, with
-// a workspace allocated on the stream for the call (stream-ordered, so calls
-// on different streams never share one); no_alloc: nothing is allocated and
-// items run whole.
+// rows of C). Allocates nothing.
 int run_jobs_with_events(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                         cudaStream_t s, void *const *events, bool no_alloc = false);
+                         cudaStream_t s, void *const *events);
 
 // tca_plan_create with two extra controls for the host-buffer forward:
 // vals_ready (an event after which the values may be read; NULL: at once)
@@ -191,9 +172,8 @@ int plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f
                 const tca_plan_opts_t *opts, cudaStream_t stream, cudaEvent_t vals_ready, bool sync_end,
                 tca_plan_t *plan);
 
-// The N-slice width a single forward of this plan uses (split: the launch
-// cuts items by chunk ranges).
-int pick_tc_tile(const tca_plan *p, int N, bool batched, bool f8 = false, bool split = true);
+// The N-slice width a single forward of this plan uses.
+int pick_tc_tile(const tca_plan *p, int N, bool batched, bool f8 = false);
 
 // SDDMM over the plan's tensor-core windows on the tensor cores
 // (sddmm_tc.cu); dY and B with 16-byte aligned rows. The nonzeros of the

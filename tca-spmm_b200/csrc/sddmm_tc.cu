@@ -51,13 +51,14 @@ constexpr int kSdYStages = 3;    // dY ring: 128 rows x 64 n, 16 KB each
 constexpr int kSdBStages = 16;   // B ring: 64 rows x 64 n, 8 KB each
 constexpr int kSdYBytes = kWindowRows * 64 * 2;
 constexpr int kSdBBytes = kChunkCols * 64 * 2;
-constexpr int kSdStageRow = 68;  // floats per row of the epilogue's staging tile (64 + 4: fewer bank conflicts)
+constexpr int kSdStageRow = 68;  // floats per row of the epilogue's staging tiles (64 + 4: fewer bank conflicts)
+constexpr int kSdStageChunks = 4; // chunks staged at once in the epilogue
 constexpr int kSdYOff = 0;
 constexpr int kSdBOff = kSdYOff + kSdYStages * kSdYBytes;
 constexpr int kSdBarOff = kSdBOff + kSdBStages * kSdBBytes;
 // y_full, y_empty [kSdYStages]; b_full, b_empty [kSdBStages]; acc_full; drain; TMEM slot, flag
 constexpr int kSdSmem = kSdBarOff + (2 * kSdYStages + 2 * kSdBStages + 2) * 8 + 16;
-static_assert(kSdYStages * kSdYBytes >= kWindowRows * kSdStageRow * 4, "the dY ring holds the epilogue's staging tile");
+static_assert(kSdBarOff >= kSdStageChunks * kWindowRows * kSdStageRow * 4, "the rings hold the epilogue's staging tiles");
 static_assert(kSdYBytes % 1024 == 0 && kSdBBytes % 1024 == 0, "swizzled tiles need 1024-byte alignment");
 static_assert(kSdSmem <= 227 * 1024, "shared memory budget");
 
@@ -136,6 +137,10 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
     const int ks0 = x.q * a.steps_per_part, ks1 = min(a.n_steps, ks0 + a.steps_per_part);
     int tcols = 32;
     while (tcols < x.nch * 64) tcols <<= 1;
+    // the part's n steps, each window starting at a different one, so that
+    // the windows do not read the same columns of B at once
+    const int rot = x.t % max(1, ks1 - ks0);
+    auto step_n = [&](int st) { return ks0 + (st + rot) % (ks1 - ks0); };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kSdYStages; s++) {
@@ -183,8 +188,8 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
             direct[c] = col0 >= 0 && col63 == col0 + kChunkCols - 1;
         }
         int yt = 0, bt = 0;
-        for (int ks = ks0; ks < ks1 && ok; ks++, yt++) {
-            const int n0 = ks * 64;
+        for (int st = 0; st < ks1 - ks0 && ok; st++, yt++) {
+            const int n0 = step_n(st) * 64;
             const int sy = yt % kSdYStages;
             uint32_t got = 1;
             if (lane == 0 && yt >= kSdYStages)
@@ -222,7 +227,7 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             int yt = 0, bt = 0;
-            for (int ks = ks0; ks < ks1 && ok; ks++, yt++) {
+            for (int st = 0; st < ks1 - ks0 && ok; st++, yt++) {
                 const int sy = yt % kSdYStages;
                 if (!mbar_wait(&y_full[sy], (yt / kSdYStages) & 1)) { ok = false; break; }
                 const uint32_t ys = smem_u32(smem + kSdYOff + sy * kSdYBytes);
@@ -234,7 +239,7 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
 #pragma unroll
                     for (int kk = 0; kk < 4; kk++)
                         sd_umma(tmem + (uint32_t)(c * 64), smem_desc(ys + kk * 32, 16, 1024),
-                                smem_desc(bs + kk * 32, 16, 1024), (ks > ks0 || kk > 0) ? 1u : 0u);
+                                smem_desc(bs + kk * 32, 16, 1024), (st > 0 || kk > 0) ? 1u : 0u);
                     umma_commit(&b_empty[sb]);
                 }
                 umma_commit(&y_empty[sy]);
@@ -259,36 +264,68 @@ __global__ void __launch_bounds__(kSdThreads, 1) k_sddmm_tc(const __grid_constan
             ok = false;
         } else {
             tc_fence_after();
-            // the MMAs are complete, so the dY ring is free: it holds the
-            // staging tile (row-major, kSdStageRow floats a row)
+            // The MMAs are complete, so both rings are free: they hold the
+            // staging tiles of up to kSdStageChunks chunks at a time (row-major,
+            // kSdStageRow floats a row); then the entries of those chunks --
+            // contiguous in the plan -- are read from them, four per thread in
+            // flight.
             float *stage = reinterpret_cast<float *>(smem + kSdYOff);
-            for (int c = 0; c < x.nch; c++) {
+            for (int g0 = 0; g0 < x.nch; g0 += kSdStageChunks) {
+                const int ng = min(kSdStageChunks, x.nch - g0);
+                for (int c = 0; c < ng; c++) {
 #pragma unroll
-                for (int cb = 0; cb < 4; cb++) {
-                    uint32_t r[16];
-                    tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(c * 64 + cb * 16), r);
-                    float4 *dst = reinterpret_cast<float4 *>(stage + row * kSdStageRow + cb * 16);
+                    for (int cb = 0; cb < 4; cb++) {
+                        uint32_t r[16];
+                        tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)((g0 + c) * 64 + cb * 16), r);
+                        float4 *dst = reinterpret_cast<float4 *>(stage + (c * kWindowRows + row) * kSdStageRow + cb * 16);
 #pragma unroll
-                    for (int q = 0; q < 4; q++)
-                        dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
-                                             __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
-                }
-                named_bar_sync(1, kSdEpiThreads);
-                const int c0 = __ldg(a.tile_ptr + c_first + c), c1 = __ldg(a.tile_ptr + c_first + c + 1);
-                for (int e = c0 + et; e < c1; e += kSdEpiThreads) {
-                    const uint32_t v = __ldg(a.entries + e);
-                    const float d = stage[(v >> 22) * kSdStageRow + ((v >> 16) & 63u)];
-                    if (a.parts > 1) {
-                        a.partials[(size_t)x.q * a.tc_nnz + e] = d;
-                    } else {
-                        const int j = __ldg(a.src + __ldg(a.tile_src + e));
-                        if (a.out_f16)
-                            reinterpret_cast<__half *>(a.out)[j] = __float2half_rn(a.alpha * d);
-                        else
-                            reinterpret_cast<float *>(a.out)[j] = a.alpha * d;
+                        for (int q = 0; q < 4; q++)
+                            dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                                 __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
                     }
                 }
-                named_bar_sync(1, kSdEpiThreads); // the staging tile is reused by the next chunk
+                named_bar_sync(1, kSdEpiThreads);
+                int bound[kSdStageChunks + 1];
+#pragma unroll
+                for (int c = 0; c <= kSdStageChunks; c++) bound[c] = __ldg(a.tile_ptr + c_first + g0 + min(c, ng));
+                for (int e0 = bound[0] + et; e0 < bound[kSdStageChunks]; e0 += 4 * kSdEpiThreads) {
+                    uint32_t v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int e = e0 + u * kSdEpiThreads;
+                        v[u] = e < bound[kSdStageChunks] ? __ldg(a.entries + e) : 0u;
+                    }
+                    int j[4];
+                    if (a.parts == 1) {
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            const int e = e0 + u * kSdEpiThreads;
+                            j[u] = e < bound[kSdStageChunks] ? __ldg(a.tile_src + e) : 0;
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            const int e = e0 + u * kSdEpiThreads;
+                            j[u] = e < bound[kSdStageChunks] ? __ldg(a.src + j[u]) : 0;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int e = e0 + u * kSdEpiThreads;
+                        if (e >= bound[kSdStageChunks])
+                            break;
+                        int c = 0;
+#pragma unroll
+                        for (int k = 1; k < kSdStageChunks; k++) c += e >= bound[k] ? 1 : 0;
+                        const float d = stage[(c * kWindowRows + (v[u] >> 22)) * kSdStageRow + ((v[u] >> 16) & 63u)];
+                        if (a.parts > 1)
+                            a.partials[(size_t)x.q * a.tc_nnz + e] = d;
+                        else if (a.out_f16)
+                            reinterpret_cast<__half *>(a.out)[j[u]] = __float2half_rn(a.alpha * d);
+                        else
+                            reinterpret_cast<float *>(a.out)[j[u]] = a.alpha * d;
+                    }
+                }
+                named_bar_sync(1, kSdEpiThreads); // the staging tiles are reused by the next group
             }
         }
     }

@@ -9,19 +9,9 @@
 // tile multiplies the 64 matching rows of B on the 5th-generation tensor
 // cores: D[128 x NT] (FP32, tensor memory) += A[128 x 64] * B[64 x NT].
 //
-// Work items are (job, window, NT-wide slice of N). The chunks of all items,
-// in item order, are cut into one contiguous range per CTA of equal length
-// (stream-K): a CTA's range covers the tail of one item, whole items and the
-// head of another, so that every SM gets the same number of chunks whatever
-// the item sizes. An item cut between CTAs is finished by the CTA that
-// completes its part last: the other parts leave FP32 partial tiles in a
-// workspace, the last one adds them in part order (a fixed order, so the
-// result does not depend on which CTA finishes last) and stores C; no CTA
-// waits for another. When the ranges would hold more items than a CTA's
-// table, items go to CTAs in turn instead (item i to CTA i mod grid).
-// Persistent CTAs (one per SM) stream the chunks of their segments through a
-// ring of kStages (A tile, B tile, entry staging) stages, with decoupled
-// roles:
+// Work items are (job, window, NT-wide slice of N); persistent CTAs (one per
+// SM) stream the chunks of their items through a ring of kStages (A tile,
+// B tile, entry staging) stages, with decoupled roles:
 //   * four loader warps, taking chunks in turn, move every byte through the
 //     TMA engine: the 64 B rows of the chunk -- one tiled box per 64 columns
 //     of N when its columns are 64 consecutive rows of B, else tile::gather4
@@ -63,7 +53,7 @@ constexpr int kEpiThreads = 128;     // warps 6-9: epilogue
 constexpr int kLoaderWarp1 = 10;     // warps 10..: TMA issue, chunks g = 1, 2, .. (mod kLoaders)
 constexpr int kLoaders = 4;          // loader warps, each issuing every kLoaders-th chunk
 constexpr int kThreads = 320 + (kLoaders - 1) * 32;
-constexpr int kMaxCtaItems = 32;      // work items (segments) per persistent CTA
+constexpr int kMaxCtaItems = 32;      // work items per persistent CTA
 constexpr int kEpiBar = 3;           // named barrier of the epilogue warps (1, 2: scatter groups)
 constexpr int kStagingBytes = ((kImageMinNnz + 3) * 4 + 15) & ~15; // entries of a sparse chunk, 16-byte rounded
 constexpr int kMaxJobs = 32;                                  // jobs per launch (kernel parameter space)
@@ -81,42 +71,15 @@ struct TcJob {
     void *C;
     int *status;
     int M, N, ldb, ldc, ntiles;
-    int n_win; // tensor-core windows of the plan
     float alpha, beta;
     unsigned flags;
 };
 
-// Chunk ranges (stream-K): the items' chunks, job by job, window by window,
-// N slice by N slice, are `units` chunk-units; CTA b covers units
-// [b * units / grid, (b + 1) * units / grid), starting in item
-// cta_start[b] = {job, window, N slice, chunk within the item}. A cut item's
-// parts leave partial tiles in `partials` (two slots of 128 x NT floats per
-// CTA: slot 2b for the CTA's first segment when that is cut, 2b + 1 for its
-// last; tc_slot), which spmm_tc_fixup adds up after the launch.
 struct TcBatch {
     int n_jobs;
     int item_start[kMaxJobs + 1];
-    int split;        // 1: chunk ranges (above); 0: item i to CTA i mod grid
-    long long units;
-    float *partials;
-    int *failed;      // split launches: set when a CTA gave up (zero before the launch); the sums are then skipped
-    int4 cta_start[kSMs];
     TcJob job[kMaxJobs];
 };
-
-// The cut items of a split launch: {job << 16 | N slice, tensor-core window,
-// first CTA, parts << 1 | head}, head: part 0 is its CTA's first segment.
-struct TcCuts {
-    int n;
-    int4 cut[kSMs];
-};
-
-// The CTA whose range holds chunk-unit u (ranges of units / grid, floored).
-__host__ __device__ inline int range_owner(long long u, long long units, int grid)
-{
-    return (int)(((u + 1) * grid - 1) / units);
-}
-__host__ __device__ inline long long range_lo(int b, long long units, int grid) { return (long long)b * units / grid; }
 
 using namespace ptx;
 
@@ -177,28 +140,6 @@ __device__ __forceinline__ void store8_out(float *p, const float *v, float alpha
     reinterpret_cast<float4 *>(p)[1] = make_float4(o[4], o[5], o[6], o[7]);
 }
 
-// Slot of part q of a cut item whose first part is on CTA b0 (head: that part
-// is CTA b0's first segment): part q > 0 is the first segment of CTA b0 + q.
-__host__ __device__ inline int tc_slot(int b0, int q, bool head)
-{
-    return q > 0 ? 2 * (b0 + q) : 2 * b0 + (head ? 0 : 1);
-}
-
-// E4M3 dequantisation of 16 accumulators of columns n..n+15: row scale x
-// column scale (16-byte aligned scale vectors; columns >= N read as 0).
-__device__ __forceinline__ void dequant16(float *v, float sa, const float *col_scale, int n, int N)
-{
-    const float4 *cs = reinterpret_cast<const float4 *>(col_scale + n);
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const float4 sv = (n + 4 * q < N) ? __ldg(cs + q) : make_float4(0.f, 0.f, 0.f, 0.f);
-        v[4 * q] *= sa * sv.x;
-        v[4 * q + 1] *= sa * sv.y;
-        v[4 * q + 2] *= sa * sv.z;
-        v[4 * q + 3] *= sa * sv.w;
-    }
-}
-
 // Shared memory (1024-byte aligned base): kStages x (A tile | B tile),
 // kStages entry staging buffers, per-stage chunk records, the CTA's item
 // table, mbarriers, four broadcast flags and the TMEM slot.
@@ -215,11 +156,10 @@ template <int NT, bool F8> struct TcCfg {
     static constexpr int kPendOff = kStagingOff + kStages * kStagingBytes; // int4 [kStages]: img, e0, e0a, e1
     static constexpr int kPend2Off = kPendOff + kStages * 16;              // int4 [kStages]: flags, buffer, item
     static constexpr int kItemOff = kPend2Off + kStages * 16;              // int4 [kMaxCtaItems]
-    static constexpr int kPartOff = kItemOff + kMaxCtaItems * 16; // int4 [kMaxCtaItems]: cut-item parts
-    static constexpr int kBarOff = kPartOff + kMaxCtaItems * 16;
-    // full, empty, staged [kStages]; accum_full, accum_empty [2]; drain; 4 flags, TMEM slot, segment
-    // count, epilogue flag
-    static constexpr int kSmem = kBarOff + (3 * kStages + 5) * 8 + 32;
+    static constexpr int kScaleOff = kItemOff + kMaxCtaItems * 16;         // E4M3: float [2][NT] column scales
+    static constexpr int kBarOff = kScaleOff + (F8 ? 2 * NT * 4 : 0);
+    // full, empty, staged [kStages]; accum_full, accum_empty [2]; drain; 4 flags, TMEM slot
+    static constexpr int kSmem = kBarOff + (3 * kStages + 5) * 8 + 24;
     static_assert(kSmem <= 227 * 1024, "shared memory budget");
     static_assert(kStage % 1024 == 0 && kATileBytes % 1024 == 0, "swizzled tiles need 1024-byte alignment");
     static_assert(kStagingOff % 16 == 0 && kStagingBytes % 16 == 0 && kPendOff % 16 == 0, "16-byte alignment");
@@ -280,7 +220,6 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     int4 *pend = reinterpret_cast<int4 *>(smem + Cfg::kPendOff);
     int4 *pend2 = reinterpret_cast<int4 *>(smem + Cfg::kPend2Off);
     int4 *items = reinterpret_cast<int4 *>(smem + Cfg::kItemOff);
-    int4 *parts = reinterpret_cast<int4 *>(smem + Cfg::kPartOff); // per segment: first CTA, part, parts, head flag
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + Cfg::kBarOff);
     uint64_t *empty = full + S;
     uint64_t *staged = empty + S;
@@ -289,7 +228,6 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     uint64_t *drain = acc_empty + 2;    // the MMA lane's last commit: every MMA it issued has completed
     volatile int *flag = reinterpret_cast<volatile int *>(drain + 1); // 2 slots per scatter group
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1) + 4;
-    volatile int *seg_count = reinterpret_cast<volatile int *>(drain + 1) + 5;
     constexpr int kScatterGroups = S % 2 == 0 ? 2 : 1; // two groups need an even ring (see the scatter role)
     constexpr int kGroupThreads = kScatterThreads / kScatterGroups;
 
@@ -300,9 +238,9 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int total = batch.item_start[batch.n_jobs];
-    const int rr_items = blockIdx.x < total ? min(kMaxCtaItems, (total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1) : 0;
+    const int n_items = blockIdx.x < total ? min(kMaxCtaItems, (total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1) : 0;
     if (smem_u32(smem) & 1023u) { // the swizzled tiles and TMA destinations need a 1024-byte aligned base
-        if (threadIdx.x == 0)
+        if (threadIdx.x == 0 && n_items > 0)
             atomicOr(batch.job[0].status, kStatusLayout);
         return;
     }
@@ -319,65 +257,8 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         mbar_init(drain, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (batch.split) {
-        // Warp 0 lists the segments of this CTA's chunk range: from its start
-        // item on, one segment per item the range reaches, with the item's
-        // cut (first CTA, part, number of parts) for the epilogue. The window
-        // records of the next 32 windows are loaded at once, one per lane.
-        if (warp == 0) {
-            const long long units = batch.units;
-            const int G = gridDim.x, b = blockIdx.x;
-            long long u = range_lo(b, units, G);
-            const long long hi = range_lo(b + 1, units, G);
-            const int4 st = batch.cta_start[b];
-            int j = st.x, w = st.y, t = st.z, i0 = st.w, n = 0;
-            while (u < hi && n < kMaxCtaItems && j < batch.n_jobs) {
-                const TcJob &a = batch.job[j];
-                const int4 wl = (w + lane < a.n_win) ? __ldg(a.win_info + w + lane) : make_int4(0, 0, 0, 0);
-                int l = 0;
-                while (u < hi && n < kMaxCtaItems && l < 32 && w + l < a.n_win) {
-                    const int wx = __shfl_sync(0xffffffffu, wl.x, l);
-                    const int wy = __shfl_sync(0xffffffffu, wl.y, l);
-                    const int z = __shfl_sync(0xffffffffu, wl.z, l);
-                    const long long u0 = u - i0; // the item's first unit
-                    const int cnt = (int)min((long long)(z - i0), hi - u);
-                    const int b0 = range_owner(u0, units, G), b1 = range_owner(u0 + z - 1, units, G);
-                    if (lane == 0) {
-                        items[n] = make_int4(wx, wy + i0, cnt, (j << 16) | t);
-                        parts[n] = make_int4(b0, b - b0, b1 - b0 + 1, range_lo(b0, units, G) == u0 ? 1 : 0);
-                    }
-                    n++;
-                    u += cnt;
-                    i0 = 0;
-                    if (++t == a.ntiles) { t = 0; l++; }
-                }
-                w += l;
-                if (w >= a.n_win) { j++; w = 0; }
-            }
-            if (lane == 0) {
-                // The range's last segment, when cut, is the head of an item
-                // another CTA finishes: it goes second (after the first,
-                // itself cut or whole), so that both cut parts complete early
-                // and the part that adds them up does so while this CTA's
-                // whole items still run.
-                if (n >= 3 && parts[n - 1].z > 1) {
-                    const int4 li = items[n - 1], lp = parts[n - 1];
-                    for (int k = n - 1; k > 1; k--) {
-                        items[k] = items[k - 1];
-                        parts[k] = parts[k - 1];
-                    }
-                    items[1] = li;
-                    parts[1] = lp;
-                }
-                *seg_count = n;
-                if (u < hi) // more segments than the table holds: the host sizes ranges so that this cannot be
-                    atomicOr(batch.job[0].status, kStatusTable);
-            }
-        }
-    } else if ((int)threadIdx.x < rr_items) {
+    if ((int)threadIdx.x < n_items)
         items[threadIdx.x] = decode_item(batch, blockIdx.x + threadIdx.x * gridDim.x);
-        parts[threadIdx.x] = make_int4((int)blockIdx.x, 0, 1, 1);
-    }
     if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(2 * NT)
@@ -388,7 +269,6 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int n_items = batch.split ? *seg_count : rr_items;
     bool ok = true;
     int total_chunks = 0; // of this CTA's items: every role runs over exactly these
     for (int k = 0; k < n_items; k++) total_chunks += items[k].z;
@@ -411,7 +291,9 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             if (k < n_items) {
                 const int4 it = items[k];
                 const TcJob &a = batch.job[it.w >> 16];
-                const int c = it.y + i;
+                // windows of one problem start their chunk walks at different
+                // chunks, so that they do not read the same rows of B at once
+                const int c = it.y + (i + it.x % it.z) % it.z;
                 if (lane < 16)
                     m.cols = __ldg(reinterpret_cast<const int4 *>(a.win_cols + (size_t)c * kChunkCols) + lane);
                 m.img = __ldg(a.img_idx + c);
@@ -570,22 +452,24 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         __syncwarp();
     } else {
         // ---------------- epilogue ----------------
-        // Per segment: wait for its accumulator; a whole item is stored to C
-        // (alpha, beta, E4M3 scales); a cut item's part leaves its FP32
-        // partial tile in its slot, for spmm_tc_fixup to add up after this
-        // launch.
         const int quarter = warp & 3;
-        const int row = quarter * 32 + lane; // TMEM lane = row of the window
         for (int k = 0; k < n_items; k++) {
             const int4 it = items[k];
-            const int4 pt = parts[k];
             const TcJob &a = batch.job[it.w >> 16];
             const int n0 = (it.w & 0xffff) * NT;
-            const int i = it.x * kWindowRows + row;
+            const int i = it.x * kWindowRows + quarter * 32 + lane;
             int out_row = -1;
             if (i < a.M && !((a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) && a.p_row_ptr[i + 1] == a.p_row_ptr[i]))
                 out_row = a.perm[i];
             const int b = k & 1;
+            if constexpr (F8) {
+                // the item's column scales, once, into shared memory (buffer b
+                // was last read for item k - 2, which every epilogue thread
+                // finished before the barrier of item k - 1)
+                float *sc = reinterpret_cast<float *>(smem + Cfg::kScaleOff) + b * NT;
+                for (int c = quarter * 32 + lane; c < NT; c += kEpiThreads)
+                    sc[c] = n0 + c < a.N ? __ldg(a.col_scale + n0 + c) : 0.f;
+            }
             uint32_t got = 0;
             if (lane == 0)
                 got = mbar_wait(&acc_full[b], (k >> 1) & 1) ? 1u : 0u;
@@ -593,39 +477,26 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
             // the four warps agree, so that none is left at a later barrier
             if (!named_bar_and(kEpiBar, kEpiThreads, got != 0)) { ok = false; break; }
             tc_fence_after();
-            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * NT);
-            if (pt.z > 1) {
-                float *mine = batch.partials + ((size_t)tc_slot(pt.x, pt.y, pt.w != 0) * kWindowRows + row) * NT;
-                for (int cb = 0; cb < NT / 16; cb++) {
-                    if (n0 + cb * 16 >= a.N)
-                        break; // uniform across the warp
-                    uint32_t r[16];
-                    tmem_ld16(taddr + cb * 16, r);
-                    float4 *dst = reinterpret_cast<float4 *>(mine + cb * 16);
+            OutT *Crow = out_row >= 0 ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
+            float sa = 1.f;
+            if constexpr (F8)
+                sa = (i < a.M) ? a.row_scale[i] : 0.f;
+            for (int cb = 0; cb < NT / 16; cb++) {
+                const int n = n0 + cb * 16;
+                if (n >= a.N)
+                    break; // uniform across the warp
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * NT + cb * 16), r);
+                if constexpr (F8) { // dequantise: row scale x column scale (staged above; the barrier orders it)
+                    float *f = reinterpret_cast<float *>(r);
+                    const float *sb = reinterpret_cast<const float *>(smem + Cfg::kScaleOff) + b * NT + cb * 16;
 #pragma unroll
-                    for (int q = 0; q < 4; q++)
-                        dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
-                                             __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+                    for (int q = 0; q < 16; q++) f[q] *= sa * sb[q];
                 }
-            } else {
-                OutT *Crow = out_row >= 0 ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
-                float sa = 1.f;
-                if constexpr (F8)
-                    sa = (i < a.M) ? a.row_scale[i] : 0.f;
-                for (int cb = 0; cb < NT / 16; cb++) {
-                    const int n = n0 + cb * 16;
-                    if (n >= a.N)
-                        break; // uniform across the warp
-                    uint32_t r[16];
-                    tmem_ld16(taddr + cb * 16, r);
-                    float *v = reinterpret_cast<float *>(r);
-                    if constexpr (F8)
-                        dequant16(v, sa, a.col_scale, n, a.N);
-                    if (Crow) {
-                        store8_out(Crow + n, v, a.alpha, a.beta);
-                        if (n + 8 < a.N)
-                            store8_out(Crow + n + 8, v + 8, a.alpha, a.beta);
-                    }
+                if (Crow) {
+                    store8_out(Crow + n, reinterpret_cast<const float *>(r), a.alpha, a.beta);
+                    if (n + 8 < a.N)
+                        store8_out(Crow + n + 8, reinterpret_cast<const float *>(r) + 8, a.alpha, a.beta);
                 }
             }
             tc_fence_before();
@@ -642,8 +513,6 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
         if (threadIdx.x == 0) {
             if (n_items > 0)
                 atomicOr(batch.job[items[0].w >> 16].status, kStatusTimeout);
-            if (batch.split)
-                atomicOr(batch.failed, 1); // its cut parts may be missing: no sums after this launch
             const uint64_t t0 = global_ns();
             while (global_ns() - t0 < 1000000ull) {
             }
@@ -653,68 +522,6 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     if (warp == kMmaWarp) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * NT) : "memory");
-    }
-}
-
-// After a split launch: block (c, r) adds up the parts of cut item c for
-// rows 32 r .. 32 r + 31 of its window, in part order -- a fixed order, so the
-// result does not depend on which CTA computed which part when -- and stores
-// C as the tensor-core epilogue stores a whole item (E4M3 scales, alpha,
-// beta, rows without nonzeros kept on request). A thread takes 8 columns of a
-// row; the loads of up to four parts are issued before the first is added.
-template <int NT, typename OutT, bool F8>
-__global__ void __launch_bounds__(256)
-spmm_tc_fixup(const __grid_constant__ TcBatch batch, const __grid_constant__ TcCuts cuts)
-{
-    if (*(volatile const int *)batch.failed)
-        return; // a CTA of the launch gave up (its status word says so): C keeps what it had
-    const int4 cu = cuts.cut[blockIdx.x];
-    const TcJob &a = batch.job[cu.x >> 16];
-    const int n0 = (cu.x & 0xffff) * NT;
-    const int window = __ldg(&a.win_info[cu.y].x);
-    const int b0 = cu.z, parts = cu.w >> 1;
-    const bool head = (cu.w & 1) != 0;
-    const int vpr = min(NT, a.N - n0) >> 3; // 8-column vectors a row (N % 8 == 0 on this path)
-    for (int idx = threadIdx.x; idx < 32 * vpr; idx += blockDim.x) {
-        const int rl = blockIdx.y * 32 + idx / vpr, c8 = (idx % vpr) * 8;
-        const int i = window * kWindowRows + rl;
-        if (i >= a.M)
-            continue;
-        const size_t off = (size_t)rl * NT + c8;
-        float acc[8];
-        for (int q0 = 0; q0 < parts; q0 += 4) {
-            float4 x[4][2];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                if (q0 + u < parts) {
-                    const float4 *src = reinterpret_cast<const float4 *>(
-                        batch.partials + (size_t)tc_slot(b0, q0 + u, head) * kWindowRows * NT + off);
-                    x[u][0] = __ldcg(src);
-                    x[u][1] = __ldcg(src + 1);
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                if (q0 + u < parts) {
-                    const float e[8] = {x[u][0].x, x[u][0].y, x[u][0].z, x[u][0].w,
-                                        x[u][1].x, x[u][1].y, x[u][1].z, x[u][1].w};
-#pragma unroll
-                    for (int k = 0; k < 8; k++) acc[k] = (q0 + u == 0) ? e[k] : acc[k] + e[k];
-                }
-            }
-        }
-        if ((a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) && a.p_row_ptr[i + 1] == a.p_row_ptr[i])
-            continue;
-        const int n = n0 + c8;
-        if constexpr (F8) {
-            const float sa = a.row_scale[i];
-            const float4 s0 = __ldg(reinterpret_cast<const float4 *>(a.col_scale + n));
-            const float4 s1 = __ldg(reinterpret_cast<const float4 *>(a.col_scale + n) + 1);
-            const float sb[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
-#pragma unroll
-            for (int k = 0; k < 8; k++) acc[k] *= sa * sb[k];
-        }
-        store8_out(reinterpret_cast<OutT *>(a.C) + (size_t)a.perm[i] * a.ldc + n, acc, a.alpha, a.beta);
     }
 }
 
@@ -800,132 +607,57 @@ int make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT,
     j.ldb = sj.ldb;
     j.ldc = sj.ldc;
     j.ntiles = (sj.N + NT - 1) / NT;
-    j.n_win = p->n_tc;
     j.alpha = alpha;
     j.beta = beta;
     j.flags = flags;
     return TCA_OK;
 }
 
-// Chunk ranges (stream-K) for a batch whose jobs' plans are `plans`: the grid
-// (at most one CTA per SM, at least kMinUnits chunks each, so that a cut item
-// has few parts to add up) and each CTA's start item, from the plans' host
-// copies of their windows' chunk offsets. False when some CTA's range would
-// reach more items than its work table holds (then items go to CTAs in turn).
-constexpr int kMinUnits = 8;
-
-bool plan_ranges(TcBatch &b, const tca_plan *const *plans, int *grid_out, TcCuts *cuts)
-{
-    cuts->n = 0;
-    long long units = 0;
-    for (int j = 0; j < b.n_jobs; j++)
-        units += (long long)plans[j]->n_tc_chunks * b.job[j].ntiles;
-    if (units <= 0)
-        return false;
-    const int G = (int)std::min<long long>(kSMs, std::max<long long>(1, units / kMinUnits));
-    int segs[kSMs] = {0};
-    long long u0 = 0;
-    for (int j = 0; j < b.n_jobs; j++) {
-        const std::vector<int> &first = plans[j]->h_tile_first;
-        for (int w = 0; w < b.job[j].n_win; w++) {
-            const int z = first[w + 1] - first[w];
-            for (int t = 0; t < b.job[j].ntiles; t++, u0 += z) {
-                const int c0 = range_owner(u0, units, G), c1 = range_owner(u0 + z - 1, units, G);
-                if (c1 > c0) {
-                    if (cuts->n == kSMs)
-                        return false; // cannot happen: a cut needs a range boundary inside the item
-                    const int head = range_lo(c0, units, G) == u0 ? 1 : 0;
-                    cuts->cut[cuts->n++] = make_int4((j << 16) | t, w, c0, ((c1 - c0 + 1) << 1) | head);
-                }
-                for (int c = c0; c <= c1; c++) {
-                    if (++segs[c] > kMaxCtaItems)
-                        return false;
-                    const long long lo = range_lo(c, units, G);
-                    if (lo >= u0)
-                        b.cta_start[c] = make_int4(j, w, t, (int)(lo - u0));
-                }
-            }
-        }
-    }
-    b.split = 1;
-    b.units = units;
-    *grid_out = G;
-    return true;
-}
-
 template <int NT, typename OutT, bool F8>
-int launch_group(const TcBatch &b, int grid, cudaStream_t s)
+int launch_group(const TcBatch &b, cudaStream_t s)
 {
     const int smem = TcCfg<NT, F8>::kSmem;
     TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int total = b.item_start[b.n_jobs];
+    const int grid = std::min(total, std::max(kSMs, (total + kMaxCtaItems - 1) / kMaxCtaItems));
     spmm_tc_kernel<NT, OutT, F8><<<grid, kThreads, smem, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
 }
 
-template <int NT, typename OutT, bool F8>
-int launch_fixup(const TcBatch &b, const TcCuts &c, cudaStream_t s)
-{
-    spmm_tc_fixup<NT, OutT, F8><<<dim3((unsigned)c.n, kWindowRows / 32), 256, 0, s>>>(b, c);
-    TCA_CUDA_TRY(cudaGetLastError());
-    return TCA_OK;
-}
-
 template <typename OutT>
-int launch_fixup_out(const TcBatch &b, const TcCuts &c, int NT, bool f8, cudaStream_t s)
+int launch_group_out(const TcBatch &b, int NT, bool f8, cudaStream_t s)
 {
     if (f8)
-        return NT == 128 ? launch_fixup<128, OutT, true>(b, c, s) : launch_fixup<256, OutT, true>(b, c, s);
+        return NT == 128 ? launch_group<128, OutT, true>(b, s) : launch_group<256, OutT, true>(b, s);
     switch (NT) {
-    case 64: return launch_fixup<64, OutT, false>(b, c, s);
-    case 128: return launch_fixup<128, OutT, false>(b, c, s);
-    default: return launch_fixup<256, OutT, false>(b, c, s);
+    case 64: return launch_group<64, OutT, false>(b, s);
+    case 128: return launch_group<128, OutT, false>(b, s);
+    default: return launch_group<256, OutT, false>(b, s);
     }
 }
 
-template <typename OutT>
-int launch_group_out(const TcBatch &b, int NT, bool f8, int grid, cudaStream_t s)
-{
-    if (f8)
-        return NT == 128 ? launch_group<128, OutT, true>(b, grid, s) : launch_group<256, OutT, true>(b, grid, s);
-    switch (NT) {
-    case 64: return launch_group<64, OutT, false>(b, grid, s);
-    case 128: return launch_group<128, OutT, false>(b, grid, s);
-    default: return launch_group<256, OutT, false>(b, grid, s);
-    }
-}
-
-int launch_group_typed(const TcBatch &b, int NT, bool f8, int c_dtype, int grid, cudaStream_t s)
+int launch_group_typed(const TcBatch &b, int NT, bool f8, int c_dtype, cudaStream_t s)
 {
     if (b.n_jobs == 0 || b.item_start[b.n_jobs] == 0)
         return TCA_OK;
-    return c_dtype == TCA_DTYPE_F16 ? launch_group_out<__half>(b, NT, f8, grid, s)
-                                    : launch_group_out<float>(b, NT, f8, grid, s);
+    return c_dtype == TCA_DTYPE_F16 ? launch_group_out<__half>(b, NT, f8, s) : launch_group_out<float>(b, NT, f8, s);
 }
 
 } // namespace
 
-int pick_tc_tile(const tca_plan *p, int N, bool batched, bool f8, bool split)
+int pick_tc_tile(const tca_plan *p, int N, bool batched, bool f8)
 {
+    const int n_tc = p->n_tc;
     const int lo = f8 ? 128 : 64; // E4M3 B tiles are whole 128-byte swizzle atoms
     int NT = N <= 64 ? 64 : N <= 128 ? 128 : 256;
     NT = std::max(NT, lo);
-    if (batched)
-        return NT;
-    if (split) {
-        // chunk ranges: halve the slice while the forward has fewer chunks
-        // than kMinUnits per SM (a wider slice's chunk carries more work, but
-        // fewer CTAs would share the forward)
-        while (NT > lo && (long long)p->n_tc_chunks * ((N + NT - 1) / NT) < (long long)kMinUnits * kSMs)
+    // a single forward halves the slice while that leaves fewer than about
+    // three quarters of the SMs with an item (measured: A^T of 512 x 2048,
+    // N = 4096, 4 windows: NT = 128, 128 items, 30.5 us; NT = 64, 40.4 us)
+    if (!batched)
+        while (NT > lo && (long long)n_tc * ((N + NT - 1) / NT) < (3 * kSMs) / 4)
             NT /= 2;
-    } else {
-        // items to CTAs in turn: halve the slice while that leaves fewer than
-        // about three quarters of the SMs with an item (measured: A^T of
-        // 512 x 2048, N = 4096, 4 windows: NT = 128, 128 items, 30.5 us;
-        // NT = 64, 40.4 us)
-        while (NT > lo && (long long)p->n_tc * ((N + NT - 1) / NT) < (3 * kSMs) / 4)
-            NT /= 2;
-    }
     return NT;
 }
 
@@ -960,47 +692,21 @@ int tc_block_regs(bool f8, int *regs)
 }
 
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
-                   cudaStream_t s, LaunchList *defer, TcWorkspace *ws, LaunchList *post)
+                   cudaStream_t s, LaunchList *defer)
 {
     const int widths[3] = {64, 128, 256};
-    auto emit = [&](TcBatch &b, const tca_plan *const *plans, int NT, bool f8) -> int {
+    auto emit = [&](const TcBatch &b, int NT, bool f8) -> int {
         if (b.n_jobs == 0 || b.item_start[b.n_jobs] == 0)
             return TCA_OK;
-        const int total = b.item_start[b.n_jobs];
-        int grid = std::min(total, std::max(kSMs, (total + kMaxCtaItems - 1) / kMaxCtaItems));
-        b.split = 0;
-        b.units = 0;
-        b.partials = nullptr;
-        b.failed = nullptr;
-        auto cuts = std::make_shared<TcCuts>();
-        cuts->n = 0;
-        size_t offset = 0; // this launch's partial tiles in the workspace (floats)
-        if (ws && defer && post && plan_ranges(b, plans, &grid, cuts.get())) {
-            offset = ws->partial_bytes / sizeof(float);
-            // every launch of the call has a region of its own: the fixups run after all of them
-            ws->partial_bytes += sizeof(float) * 2 * (size_t)grid * kWindowRows * NT;
-        }
         if (!defer)
-            return launch_group_typed(b, NT, f8, c_dtype, grid, s);
+            return launch_group_typed(b, NT, f8, c_dtype, s);
         auto held = std::make_shared<TcBatch>(b);
-        defer->push_back([held, NT, f8, c_dtype, grid, ws, offset](cudaStream_t st) {
-            if (held->split) {
-                held->partials = ws->partials + offset;
-                held->failed = ws->failed;
-            }
-            return launch_group_typed(*held, NT, f8, c_dtype, grid, st);
-        });
-        if (held->split && cuts->n > 0)
-            post->push_back([held, cuts, NT, f8, c_dtype](cudaStream_t st) {
-                return c_dtype == TCA_DTYPE_F16 ? launch_fixup_out<__half>(*held, *cuts, NT, f8, st)
-                                                : launch_fixup_out<float>(*held, *cuts, NT, f8, st);
-            });
+        defer->push_back([held, NT, f8, c_dtype](cudaStream_t st) { return launch_group_typed(*held, NT, f8, c_dtype, st); });
         return TCA_OK;
     };
     for (bool f8 : {false, true}) {
         for (int NT : widths) {
             TcBatch b;
-            const tca_plan *plans[kMaxJobs];
             b.n_jobs = 0;
             b.item_start[0] = 0;
             for (int i = 0; i < n_jobs; i++) {
@@ -1008,15 +714,14 @@ int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
                 if (!sj.tc || sj.f8 != f8 || sj.n_tile != NT || sj.p->n_tc == 0 || sj.N <= 0)
                     continue;
                 TCA_TRY(make_job(sj, alpha, beta, flags, NT, &b.job[b.n_jobs]));
-                plans[b.n_jobs] = sj.p;
                 b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + sj.p->n_tc * b.job[b.n_jobs].ntiles;
                 b.n_jobs++;
                 if (b.n_jobs == kMaxJobs) {
-                    TCA_TRY(emit(b, plans, NT, f8));
+                    TCA_TRY(emit(b, NT, f8));
                     b.n_jobs = 0;
                 }
             }
-            TCA_TRY(emit(b, plans, NT, f8));
+            TCA_TRY(emit(b, NT, f8));
         }
     }
     return TCA_OK;

@@ -244,12 +244,11 @@ def test_full_size_configs(cuda, cfg):
 
 
 @pytest.mark.parametrize("M,K,N,d", [(256, 8192, 64, 0.3), (1000, 4096, 136, 0.2), (300, 2048, 512, 0.5)])
-def test_items_cut_across_ctas(cuda, M, K, N, d):
-    """Few windows with many chunks each: the launch cuts every item into
-    parts on several CTAs (chunk ranges), and the part that arrives last adds
-    the others' partial tiles in part order. FP32 and FP16 outputs within the
-    tolerances above, E4M3 within 2e-5 of the FP64 product of its dequantized
-    operands, and two launches identical bit for bit."""
+def test_long_windows(cuda, M, K, N, d):
+    """Few windows with many chunks each (long items on few CTAs, wide K,
+    N beyond one slice): FP32 and FP16 outputs within the tolerances above,
+    E4M3 within 2e-5 of the FP64 product of its dequantized operands, and two
+    launches identical bit for bit."""
     c = gen.small(np.random.default_rng(M + K), M, K, N, d, empty_rows=0.05)
     rp, ci, v, B = dev(c, cuda)
     plan = tca_spmm.Plan(rp, ci, v, c["K"])
