@@ -224,8 +224,8 @@ TCA_API int tca_plan_launch_counts(tca_plan_t plan, int N, int *n_tc_launches, i
 /* ---- FP8-E4M3 forward (no counterpart in the reference, which computes in
  * FP16 only; src/our_spmm.cu:109-145 uses FP16 mma.sync) ----
  * A is quantized per sorted row, B per column: s = max|x| / 448 (1 for an
- * all-zero row or column), q = E4M3(x / s) rounded to nearest even and
- * saturated. The forward accumulates the exact products q_a * q_b in FP32 and
+ * all-zero row or column), q = E4M3(x / s) for A and q = E4M3(x * r) with
+ * r = 1 / s rounded to FP32 for B, rounded to nearest even and saturated. The forward accumulates the exact products q_a * q_b in FP32 and
  * returns alpha * (sum * s_a[row] * s_b[col]) + beta * C. */
 
 /* Builds (or, after new values, refreshes) the plan's E4M3 form of A.
@@ -302,8 +302,11 @@ TCA_API int tca_batch_graph_create_events(const tca_batch_item_t *items, int n_i
 TCA_API int tca_batch_graph_launch(tca_graph_t graph, tca_stream_t stream);
 TCA_API int tca_batch_graph_destroy(tca_graph_t graph);
 /* Per item, times every (n_tile, cc_cols) candidate on the item alone (median
- * of `reps` runs, CUDA events on `stream`, synchronising) and stores the
- * fastest into items[i].n_tile / items[i].cc_cols. Writes the items' C. */
+ * of `reps` runs, CUDA events on `stream`, synchronising); then, for batches
+ * of more than one item, times those picks as a whole against every uniform
+ * (n_tile, cc_cols) for all items, each as replays of a captured graph, and
+ * stores the fastest into items[i].n_tile / items[i].cc_cols. Writes the
+ * items' C. */
 TCA_API int tca_batch_autotune(tca_batch_item_t *items, int n_items, int c_dtype, int precision, int reps,
                                tca_stream_t stream);
 

@@ -611,8 +611,13 @@ void orc_quant_cols(int K, int N, const uint16_t *B, int ldb, uint8_t *q, int ld
         }
         scale[n] = orc_scale_of(m);
     }
+    /* B is divided by its column scale as a product with the FP32 reciprocal
+     * (one correctly rounded division per column, as the GPU kernels do) */
     for (int k = 0; k < K; k++)
-        for (int n = 0; n < N; n++) q[(size_t)k * ldq + n] = orc_f32_to_e4m3(orc_h2f(B[(size_t)k * ldb + n]) / scale[n]);
+        for (int n = 0; n < N; n++) {
+            const float inv = 1.0f / scale[n];
+            q[(size_t)k * ldq + n] = orc_f32_to_e4m3(orc_h2f(B[(size_t)k * ldb + n]) * inv);
+        }
 }
 
 /* ---------------------------------------------------------------------------

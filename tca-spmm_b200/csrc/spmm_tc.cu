@@ -618,6 +618,13 @@ int launch_group(const TcBatch &b, cudaStream_t s)
 {
     const int smem = TcCfg<NT, F8>::kSmem;
     TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    // The whole 228 KB carveout: with the smallest one that holds this block
+    // (196 KB for the E4M3 rings) no room is left for the 1 KB that each
+    // CUDA-core block reserves, and the launch that should run beside this
+    // one waits for it to end (measured: E4M3 step, CUDA-core blocks starting
+    // as the first tensor-core blocks exit).
+    TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT, F8>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
     const int total = b.item_start[b.n_jobs];
     const int grid = std::min(total, std::max(kSMs, (total + kMaxCtaItems - 1) / kMaxCtaItems));
     spmm_tc_kernel<NT, OutT, F8><<<grid, kThreads, smem, s>>>(b);

@@ -412,8 +412,9 @@ def _batch_items(plans, Bs, outs, n_tiles=None, cc_cols=None):
 
 
 def autotune(plans, Bs, outs, precision="f16", reps=5, stream=None):
-    """Per item, the fastest (n_tile, cc_cols) by timing every candidate on the
-    item alone (tca_batch_autotune). Overwrites `outs`."""
+    """The fastest (n_tile, cc_cols) per item (tca_batch_autotune): every
+    candidate timed on the item alone, then those picks timed as one batch
+    against each uniform configuration for all items. Overwrites `outs`."""
     arr = _batch_items(plans, Bs, outs)
     code = _out_code(outs[0].dtype) if plans else DTYPE_F16
     _check(lib().tca_batch_autotune(arr, len(plans), code, _PRECISIONS[precision], reps, _stream_handle(stream)))

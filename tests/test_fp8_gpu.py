@@ -99,10 +99,12 @@ def test_fp8_forward_vs_dequantized_f64(cuda, case, path, N, out_dtype):
     assert err <= (2e-5 if out_dtype == "f32" else 1e-3), err
 
 
-@pytest.mark.parametrize("K,N", [(300, 2048), (257, 2047), (64, 9472), (1024, 1184)])
+@pytest.mark.parametrize("K,N", [(300, 2048), (257, 2047), (64, 9472), (1024, 1184), (2000, 1300), (8192, 1200)])
 def test_b_quantization_one_launch_bit_exact(cuda, K, N):
     """Wide B (enough column strips for the one-launch quantization, several
-    strip widths, a ragged last strip) against the oracle, bit for bit."""
+    strip widths, a ragged last strip; strips held in shared memory, and --
+    K = 8192 -- strips too tall for it, read twice) against the oracle, bit
+    for bit."""
     rng = np.random.default_rng(K + N)
     B = (rng.standard_normal((K, N)) * rng.choice([1e-3, 1.0, 50.0], N)).astype(np.float16)
     B[:, 3] = 0  # an all-zero column: scale 1
