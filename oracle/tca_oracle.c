@@ -517,13 +517,13 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
         }
         p->tile_ptr[c0 + nch[w]] = (int)base;
     }
-    /* chunks with >= 2048 entries also become a dense 128 x 64 FP16 tile in
+    /* chunks with >= 512 entries (1/16 of the tile) also become a dense 128 x 64 FP16 tile in
      * the 128-byte swizzled K-major layout: element (r, c) at byte
      * r*128 + ((c/8) ^ (r%8))*16 + (c%8)*2 */
     p->img_idx = (int *)malloc(sizeof(int) * ((size_t)p->n_tc_chunks + 1));
     p->n_images = 0;
     for (int c = 0; c < p->n_tc_chunks; c++)
-        p->img_idx[c] = (p->tile_ptr[c + 1] - p->tile_ptr[c] >= WR * CW / 4) ? p->n_images++ : -1;
+        p->img_idx[c] = (p->tile_ptr[c + 1] - p->tile_ptr[c] >= WR * CW / 16) ? p->n_images++ : -1;
     p->images = (uint16_t *)calloc((size_t)p->n_images * WR * CW + 1, sizeof(uint16_t));
     for (int c = 0; c < p->n_tc_chunks; c++) {
         if (p->img_idx[c] < 0) continue;

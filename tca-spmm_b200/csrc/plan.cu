@@ -21,7 +21,7 @@
 //      per chunk (one block each) the nonzeros of every row inside the chunk
 //      -- counted, prefix-summed into tile_ptr, written as entries packed
 //      (local_row << 22 | local_col << 16 | fp16 bits) ordered by (row, col);
-//   6. dense 16 KB images of the chunks with >= 2048 entries; CUDA-core
+//   6. dense 16 KB images of the chunks with >= 512 entries; CUDA-core
 //      work items (host).
 #include <cub/cub.cuh>
 #include <vector>
@@ -626,7 +626,7 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         TCA_CUDA_TRY(cudaMemsetAsync(p->tile_ptr, 0, sizeof(int), s));
     }
 
-    // 6. dense tile images for chunks holding at least half a tile of nonzeros
+    // 6. dense tile images for chunks holding at least kImageMinNnz nonzeros
     std::vector<int> h_ptr((size_t)p->n_tc_chunks + 1, 0), h_img((size_t)p->n_tc_chunks, -1), h_img_chunk;
     if (p->n_tc_chunks > 0)
         TCA_CUDA_TRY(cudaMemcpyAsync(h_ptr.data(), p->tile_ptr, sizeof(int) * h_ptr.size(), cudaMemcpyDeviceToHost, s));

@@ -18,9 +18,9 @@
 //                      tile_src indexes p_val; 4 zero entries of padding let
 //                      16-byte copies round the end of the last chunk up
 //   img_idx[chunks], images[n_images * 8192] (FP16)
-//                      chunks with >= 2048 nonzeros (a quarter of the tile:
-//                      at most twice the bytes of their entries, and no
-//                      scatter work) are also kept
+//                      chunks with >= 512 nonzeros (1/16 of the tile: at
+//                      most 8x the bytes of their entries, and no scatter
+//                      work on the kernel's critical path) are also kept
 //                      as a dense 128 x 64 tile, already in the 128-byte
 //                      swizzled K-major layout the tensor cores read from
 //                      shared memory; img_idx is -1 for the other chunks
@@ -86,7 +86,15 @@ struct tca_plan {
 
 namespace tca {
 
-constexpr int kImageMinNnz = kWindowRows * kChunkCols / 4; // 2048
+// Chunks with at least this many nonzeros (1/16 of the tile) also get a
+// pre-rendered dense image, which the tensor-core kernel loads with one bulk
+// copy instead of scattering entries: the scatter sits on the chunk's
+// critical path, while the image's extra HBM bytes (16 KB, up to 8x the
+// entries of such a chunk) do not bound the kernel (measured on the
+// 32-problem step at 80 %, threshold 2048 -> 512: FP16 tensor-core kernel
+// 53.0 -> 50.4 us, E4M3 43.0 -> 36.9 us; 128 gave 50.1 us for twice the
+// image memory of the sparsest chunks).
+constexpr int kImageMinNnz = kWindowRows * kChunkCols / 16; // 512
 constexpr int kEntryPad = 4;
 constexpr int kItemRows = 31;
 constexpr int kItemNnz = 32;

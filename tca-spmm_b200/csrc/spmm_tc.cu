@@ -18,7 +18,7 @@
 //     of the condensed columns (4 rows x 128 bytes per instruction into a
 //     128-byte swizzled N-major tile; padding columns and n >= N are out of
 //     the tensor and arrive as zeros) -- and either the chunk's pre-rendered,
-//     pre-swizzled dense A tile (chunks with >= 2048 nonzeros: one 16 KB
+//     pre-swizzled dense A tile (chunks with >= 512 nonzeros: one 16 KB
 //     cp.async.bulk) or its packed entries (cp.async.bulk into the stage's
 //     staging buffer);
 //   * scatter warps (two groups taking chunks in turn), once a stage's
@@ -149,7 +149,7 @@ template <int NT, bool F8> struct TcCfg {
     static constexpr int kElem = F8 ? 1 : 2;
     static constexpr int kATileBytes = kWindowRows * kChunkCols * kElem;
     static constexpr int kBoxCols = 128 / kElem; // N columns per 128-byte swizzle atom / TMA box
-    static constexpr int kStages = F8 ? (NT == 256 ? 6 : 8) : (NT == 256 ? 4 : NT == 128 ? 5 : 6);
+    static constexpr int kStages = F8 ? (NT == 256 ? 8 : 12) : (NT == 256 ? 4 : NT == 128 ? 6 : 8);
     static constexpr int kBTileBytes = kChunkCols * NT * kElem;
     static constexpr int kStage = kATileBytes + kBTileBytes;
     static constexpr int kStagingOff = kStages * kStage;

@@ -71,13 +71,13 @@ def unswizzle(img):
 
 
 def check_images(p):
-    """Every chunk with >= 2048 entries has an image equal to its entries."""
+    """Every chunk with >= 512 entries (1/16 of the tile) has an image equal to its entries."""
     ptr = p["tile_ptr"]
     n_img = 0
     for ch in range(p["n_tc_chunks"]):
         cnt = ptr[ch + 1] - ptr[ch]
         idx = p["tile_image_idx"][ch]
-        assert (idx >= 0) == (cnt >= 2048)
+        assert (idx >= 0) == (cnt >= 512)
         if idx < 0:
             continue
         assert idx == n_img
