@@ -103,7 +103,11 @@ typedef struct tca_plan_opts {
     int sort_rows;        /* 1 (default): windows over rows sorted by nnz; 0: natural row order */
     float tc_min_density; /* windows with condensed density >= this use tensor cores (default 0.02) */
     int path;             /* 0 auto (default), 1 CUDA cores only, 2 tensor cores only */
-    int reserved[5];
+    int pair_windows;     /* 0 (default): one tensor-core window per SM; 1: consecutive windows
+                             with identical chunk columns run as pairs on two SMs (tcgen05
+                             cta_group::2) for N-slices of 256 -- correct, but measured slower on
+                             the sweep problems (FP16 kernel 63 vs 50 us, E4M3 59 vs 37 us) */
+    int reserved[4];
 } tca_plan_opts_t;
 
 typedef struct tca_plan_info {
@@ -138,7 +142,8 @@ typedef enum tca_plan_array {
     TCA_ARR_ROW_SCALE = 16,   /* [float, M] E4M3 scale per sorted row (after tca_plan_quantize_fp8) */
     TCA_ARR_P_VAL_F8 = 17,    /* [u8, nnz] E4M3 values, sorted order */
     TCA_ARR_TILE_ENTRIES_F8 = 18, /* [u32] tile entries with the E4M3 value in the low byte */
-    TCA_ARR_TILE_IMAGES_F8 = 19   /* [u8, n_images*8192] dense 128x64 E4M3 tiles, 64-byte swizzled K-major */
+    TCA_ARR_TILE_IMAGES_F8 = 19,  /* [u8, n_images*8192] dense 128x64 E4M3 tiles, 64-byte swizzled K-major */
+    TCA_ARR_TC_PAIRS = 20     /* [int pairs] tensor-core window pairs (indices into TCA_ARR_TC_WINDOWS; second -1: alone) */
 } tca_plan_array_t;
 
 TCA_API void tca_plan_opts_default(tca_plan_opts_t *opts);

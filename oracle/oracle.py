@@ -33,7 +33,8 @@ class OrcPlan(ctypes.Structure):
                 ("tc_windows", _P), ("cc_windows", _P), ("tile_first", _P), ("win_cols", _P),
                 ("tile_ptr", _P), ("tile_src", _P), ("tile_entries", _P),
                 ("n_images", _I), ("img_idx", _P), ("images", _P),
-                ("n_cc_items", _I), ("n_all_items", _I), ("cc_items", _P), ("all_items", _P)]
+                ("n_cc_items", _I), ("n_all_items", _I), ("cc_items", _P), ("all_items", _P),
+                ("n_pairs", _I), ("tc_pairs", _P)]
 
 
 _lib = None
@@ -203,6 +204,7 @@ def build_plan(row_ptr, col_idx, vals, K, sort_rows=True, tc_min_density=0.02, p
         tile_images=arr(p.images, p.n_images * 8192, np.uint16),
         cc_items=arr(p.cc_items, 2 * p.n_cc_items, np.int32),
         all_items=arr(p.all_items, 2 * p.n_all_items, np.int32),
+        tc_pairs=arr(p.tc_pairs, 2 * p.n_pairs, np.int32),
     )
     L.orc_plan_free(ctypes.byref(p))
     return out

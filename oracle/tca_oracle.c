@@ -350,6 +350,8 @@ typedef struct orc_plan {
     uint16_t *images;
     int n_cc_items, n_all_items;
     int *cc_items, *all_items; /* pairs [first, end) of sorted rows */
+    int n_pairs;
+    int *tc_pairs; /* [2 * n_pairs] tensor-core window index pairs, second -1 when alone */
 } orc_plan;
 
 /* CUDA-core work items over the rows of the listed windows: maximal runs of
@@ -384,7 +386,7 @@ void orc_plan_free(orc_plan *p)
     free(p->perm); free(p->p_row_ptr); free(p->p_col); free(p->src); free(p->p_val);
     free(p->tc_windows); free(p->cc_windows); free(p->tile_first); free(p->win_cols);
     free(p->tile_ptr); free(p->tile_src); free(p->tile_entries); free(p->img_idx); free(p->images);
-    free(p->cc_items); free(p->all_items);
+    free(p->cc_items); free(p->all_items); free(p->tc_pairs);
     memset(p, 0, sizeof(*p));
 }
 
@@ -437,6 +439,7 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
     int *rank = (int *)malloc(sizeof(int) * (K > 0 ? K : 1));
     int *is_tc = (int *)calloc((size_t)W, sizeof(int)), *nch = (int *)calloc((size_t)W, sizeof(int));
     int *wnnz = (int *)calloc((size_t)W, sizeof(int)), *direct = (int *)calloc((size_t)W, sizeof(int));
+    int *wblk = (int *)calloc((size_t)W, sizeof(int));
     for (int w = 0; w < W; w++) {
         int r0 = w * WR, r1 = r0 + WR < M ? r0 + WR : M;
         int lo = p->p_row_ptr[r0], hi = p->p_row_ptr[r1];
@@ -457,6 +460,7 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
          * most twice the chunks of the condensed distinct columns */
         int nch_cond = (nu + CW - 1) / CW;
         direct[w] = nblk <= 2 * nch_cond;
+        wblk[w] = nblk;
         nch[w] = direct[w] ? nblk : nch_cond;
         if (elig && wnnz[w] > 0) {
             if (path == 2) is_tc[w] = 1;
@@ -543,7 +547,23 @@ int orc_plan_build(const int *row_ptr, const int *col, const uint16_t *val, int 
     p->all_items = (int *)malloc(sizeof(int) * (2 * (size_t)p->n_all_items + 1));
     orc_build_items(all, W, p->p_row_ptr, M, p->all_items);
     free(all);
-    free(cur); free(rank); free(is_tc); free(nch); free(wnnz); free(direct); free(row_nnz); free(row_sorted);
+    /* window pairs for the pair kernel: consecutive tensor-core windows that
+     * are direct and touch every 64-column block of K have the same chunk
+     * columns; greedily paired in tensor-core order, any other window alone */
+    p->tc_pairs = (int *)malloc(sizeof(int) * (2 * (size_t)p->n_tc + 1));
+    p->n_pairs = 0;
+    {
+        const int nkb = (K + CW - 1) / CW;
+        for (int t = 0; t < p->n_tc;) {
+            int wa = p->tc_windows[t], wb = t + 1 < p->n_tc ? p->tc_windows[t + 1] : -1;
+            int fa = direct[wa] && wblk[wa] == nkb, fb = wb >= 0 && direct[wb] && wblk[wb] == nkb;
+            p->tc_pairs[2 * p->n_pairs] = t;
+            p->tc_pairs[2 * p->n_pairs + 1] = (fa && fb) ? t + 1 : -1;
+            p->n_pairs++;
+            t += (fa && fb) ? 2 : 1;
+        }
+    }
+    free(cur); free(rank); free(is_tc); free(nch); free(wnnz); free(direct); free(wblk); free(row_nnz); free(row_sorted);
     return 0;
 }
 

@@ -404,7 +404,7 @@ void free_plan(tca_plan *p)
     void *arrs[] = {p->perm, p->p_row_ptr, p->p_col, p->p_val, p->src, p->tc_windows, p->cc_windows,
                     p->all_windows, p->tile_first, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src,
                     p->img_idx, p->images, p->img_chunk, p->cc_items, p->all_items, p->tc_win_info,
-                    p->d_status};
+                    p->tc_pairs, p->d_status};
     for (void *a : arrs)
         if (a) dev_free(a, nullptr);
     delete p;
@@ -548,7 +548,8 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     // whose B rows are contiguous and load as tiled TMA boxes) when that needs
     // at most twice the chunks of condensing its distinct columns (gathered
     // B rows); otherwise condensed.
-    std::vector<int> tc_list, cc_list, h_first(1, 0), h_direct;
+    std::vector<int> tc_list, cc_list, h_first(1, 0), h_direct, h_full;
+    const int n_kblocks = (K + kChunkCols - 1) / kChunkCols;
     long long ebase = 0; // nonzeros of the tensor-core windows so far
     for (int w = 0; w < W; w++) {
         const int nch_cond = (h_nu[w] + kChunkCols - 1) / kChunkCols;
@@ -564,6 +565,7 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         if (tc) {
             tc_list.push_back(w);
             h_direct.push_back(direct ? 1 : 0);
+            h_full.push_back(direct && h_nblk[w] == n_kblocks ? 1 : 0);
             h_first.push_back(h_first.back() + nch);
             ebase += h_nnz[w];
         } else {
@@ -589,6 +591,24 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     TCA_TRY(dev_alloc(&p->tc_win_info, (size_t)p->n_tc, bytes));
     if (p->n_tc)
         TCA_CUDA_TRY(cudaMemcpyAsync(p->tc_win_info, h_wi.data(), sizeof(int4) * p->n_tc, cudaMemcpyHostToDevice, s));
+    // window pairs for the pair kernel: greedily, consecutive windows whose
+    // chunks are all 64-column blocks of K (identical columns)
+    std::vector<int2> h_pairs;
+    p->n_full_pairs = 0;
+    for (int t = 0; t < p->n_tc;) {
+        if (h_full[t] && t + 1 < p->n_tc && h_full[t + 1]) {
+            h_pairs.push_back(make_int2(t, t + 1));
+            p->n_full_pairs++;
+            t += 2;
+        } else {
+            h_pairs.push_back(make_int2(t, -1));
+            t += 1;
+        }
+    }
+    p->n_pairs = (int)h_pairs.size();
+    TCA_TRY(dev_alloc(&p->tc_pairs, (size_t)p->n_pairs, bytes));
+    if (p->n_pairs)
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->tc_pairs, h_pairs.data(), sizeof(int2) * p->n_pairs, cudaMemcpyHostToDevice, s));
 
     // 5. tiles
     TCA_TRY(dev_alloc(&p->win_cols, (size_t)p->n_tc_chunks * kChunkCols, bytes));
@@ -752,6 +772,7 @@ void tca_plan_opts_default(tca_plan_opts_t *o)
     o->sort_rows = 1;
     o->tc_min_density = 0.02f;
     o->path = 0;
+    o->pair_windows = 0;
 }
 
 int tca_plan_create(const int *d_row_ptr, const int *d_col_idx, const void *d_vals_f16, int M, int K, int nnz,
@@ -816,6 +837,7 @@ int tca_plan_export(tca_plan_t p, int which, void *h_dst, size_t capacity, size_
     case TCA_ARR_TILE_IMAGES: src = p->images; n = sizeof(uint16_t) * (size_t)p->n_images * kWindowRows * kChunkCols; break;
     case TCA_ARR_CC_ITEMS: src = p->cc_items; n = sizeof(int2) * (size_t)p->n_cc_items; break;
     case TCA_ARR_ALL_ITEMS: src = p->all_items; n = sizeof(int2) * (size_t)p->n_all_items; break;
+    case TCA_ARR_TC_PAIRS: src = p->tc_pairs; n = sizeof(int2) * (size_t)p->n_pairs; break;
     case TCA_ARR_ROW_SCALE: src = p->row_scale; n = p->has_fp8 ? sizeof(float) * (size_t)p->M : 0; break;
     case TCA_ARR_P_VAL_F8: src = p->p_val_f8; n = p->has_fp8 ? (size_t)p->nnz : 0; break;
     case TCA_ARR_TILE_ENTRIES_F8: src = p->tile_entries_f8; n = p->has_fp8 ? sizeof(uint32_t) * (size_t)p->tc_nnz : 0; break;

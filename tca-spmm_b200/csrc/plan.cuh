@@ -43,7 +43,12 @@ struct tca_plan {
     int *cc_windows = nullptr;
     int *all_windows = nullptr;
     int *tile_first = nullptr;
-    int4 *tc_win_info = nullptr; // per tensor-core window: {window, first chunk, chunk count, 0}
+    int4 *tc_win_info = nullptr; // per tensor-core window: {window, first chunk, chunk count, direct}
+    // tensor-core windows in pairs (indices into tc_windows): consecutive
+    // direct windows that touch every 64-column block of K have identical
+    // chunk columns and pair up; any other window is alone (second -1)
+    int2 *tc_pairs = nullptr;
+    int n_pairs = 0, n_full_pairs = 0;
     int *win_cols = nullptr;
     int *tile_ptr = nullptr;
     uint32_t *tile_entries = nullptr;

@@ -61,6 +61,85 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     }
 }
 
+// ---- a CTA pair (cluster of two): the partner's shared memory and barriers
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// Shared::cluster address of the object at `local` (this CTA's shared
+// memory) in the CTA of cluster rank `rank`.
+__device__ __forceinline__ uint32_t cluster_map(uint32_t local, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+    return r;
+}
+// Arrive (count 1) on an mbarrier of a CTA in the cluster, releasing this
+// thread's prior writes at cluster scope.
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_addr)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// mbar_wait for a phase completed by arrivals from the partner CTA.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_try_wait_cluster(bar, parity))
+        return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try_wait_cluster(bar, parity))
+            return true;
+        if ((it & 255u) == 0u && global_ns() - t0 > 1000000000ull)
+            return false;
+    }
+}
+// Bounded wait that polls with the non-blocking test_wait (cluster-scope
+// acquire) instead of the potentially suspending try_wait: for phases that
+// the partner CTA completes (remote arrivals, multicast commits), where a
+// suspended waiter was measured to notice the completion ~1 us late.
+__device__ __forceinline__ bool mbar_test_wait_cluster(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_poll_cluster(uint64_t *bar, uint32_t parity)
+{
+    if (mbar_test_wait_cluster(bar, parity))
+        return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_test_wait_cluster(bar, parity))
+            return true;
+        if ((it & 255u) == 0u && global_ns() - t0 > 1000000000ull)
+            return false;
+    }
+}
+
+// All threads of both CTAs of the cluster (aligned: every thread executes it).
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 __device__ __forceinline__ void named_bar_sync(int id, int n)
 {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");

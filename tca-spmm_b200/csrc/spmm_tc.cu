@@ -55,6 +55,7 @@ constexpr int kLoaders = 4;          // loader warps, each issuing every kLoader
 constexpr int kThreads = 320 + (kLoaders - 1) * 32;
 constexpr int kMaxCtaItems = 32;      // work items per persistent CTA
 constexpr int kEpiBar = 3;           // named barrier of the epilogue warps (1, 2: scatter groups)
+constexpr int kEpiWarp0 = 6;         // first epilogue warp
 constexpr int kStagingBytes = ((kImageMinNnz + 3) * 4 + 15) & ~15; // entries of a sparse chunk, 16-byte rounded
 constexpr int kMaxJobs = 32;                                  // jobs per launch (kernel parameter space)
 
@@ -62,6 +63,7 @@ struct TcJob {
     CUtensorMap tmap_b;    // B as a 2-D tensor {N, K}, box {64, 1}, 128-byte swizzle (gather4 source)
     CUtensorMap tmap_tile; // the same tensor, box {64, 64}: 64 contiguous rows of B per instruction
     const int4 *win_info; // per tensor-core window: window, first chunk, chunk count
+    const int2 *pairs;    // pair kernel: tensor-core window pairs (second -1: alone)
     const int *tile_ptr, *win_cols, *img_idx, *perm, *p_row_ptr;
     const uint32_t *entries;
     const uint8_t *images;   // dense tile images (16 KB FP16 or 8 KB E4M3 each)
@@ -525,6 +527,439 @@ __global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_const
     }
 }
 
+// ---------------------------------------------------------------------------
+// Window pairs on CTA pairs (tcgen05 cta_group::2).
+//
+// A chunk of the kernel above holds 48 KB (A tile 16 KB, B tile 64 x 256 x 2)
+// and its ring fits 4 stages; the chunk time is the ring's round trip (loads
+// land ~2 us after issue whatever their size, measured) over those 4 stages.
+// Two windows whose chunks have the same columns (direct windows that touch
+// every 64-column block of K) share every B tile, so a cluster of two CTAs on
+// two SMs runs them as one M = 256 product: each CTA loads its own window's A
+// tile and HALF of the B tile (128 of the 256 columns of N), the first CTA's
+// single MMA lane multiplies both (tcgen05.mma.cta_group::2 reads the
+// operands from both CTAs' shared memory) and each CTA's tensor memory holds
+// its own window's 128 x 256 accumulator. A stage is then 32 KB (E4M3:
+// 16 KB), so 6 (E4M3: 12) fit. A window without a partner runs with an empty
+// one (zero A tile, no stores).
+//   Opt-in (tca_plan_opts_t.pair_windows): correct, but measured slower on the
+// 32-problem sweep step (FP16 63 us against 50 us for spmm_tc_kernel, E4M3 59
+// against 37 us). Traces show each CTA's chunks completing one per ~0.9 us
+// (FP16) / ~0.65 us (E4M3) whatever the stage count (4 to 12) and however the
+// partner's completions are waited for -- half the per-SM throughput of the
+// single-window kernel -- so the halved B bytes per SM buy nothing, and 192
+// pair items on 74 CTA pairs balance worse than 352 items on 148 CTAs.
+//   Per CTA the roles are those of spmm_tc_kernel. Synchronisation between
+// the two: the second CTA's warp 5 forwards each stage's completion ("full",
+// its loads landed and scattered) to the first CTA's "peer_full"; the MMA
+// lane releases the stage in both CTAs and announces finished accumulators
+// to both epilogues with multicast commits; each epilogue reports its drained
+// accumulator to the first CTA's "acc_empty" (count 2). Every wait is bounded
+// as above; waits on phases the partner completes poll with test_wait. At
+// exit each CTA waits (bounded) until its partner has made its last access to
+// this CTA's shared memory. No load uses multicast.
+constexpr int kPairN = 256;
+
+template <bool F8> struct Tc2Cfg {
+    static constexpr int kElem = F8 ? 1 : 2;
+    static constexpr int kATileBytes = kWindowRows * kChunkCols * kElem;
+    static constexpr int kHalfCols = kPairN / 2;             // columns of N whose B rows this CTA loads
+    static constexpr int kBoxCols = 128 / kElem;             // N columns per 128-byte swizzle atom / TMA box
+    static constexpr int kBoxes = kHalfCols / kBoxCols;      // 2 (FP16) or 1 (E4M3)
+    static constexpr int kBTileBytes = kChunkCols * kHalfCols * kElem;
+    static constexpr int kStage = kATileBytes + kBTileBytes; // 32 KB / 16 KB
+    static constexpr int kStages = F8 ? 12 : 6;
+    static constexpr int kStagingOff = kStages * kStage;
+    static constexpr int kPendOff = kStagingOff + kStages * kStagingBytes;
+    static constexpr int kPend2Off = kPendOff + kStages * 16;
+    static constexpr int kItemOff = kPend2Off + kStages * 16; // int4 [kMaxCtaItems][2]
+    static constexpr int kScaleOff = kItemOff + kMaxCtaItems * 32;
+    static constexpr int kBarOff = kScaleOff + (F8 ? 2 * kPairN * 4 : 0);
+    // full, empty, staged, peer_full [kStages]; acc_full, acc_empty [2]; drain; bye; 4 flags, TMEM slot
+    static constexpr int kSmem = kBarOff + (4 * kStages + 6) * 8 + 24;
+    static_assert(kSmem <= 227 * 1024, "shared memory budget");
+    static_assert(kStage % 1024 == 0 && kATileBytes % 1024 == 0, "swizzled tiles need 1024-byte alignment");
+    static_assert(kPendOff % 16 == 0 && kItemOff % 16 == 0 && kBarOff % 16 == 0, "16-byte aligned regions");
+    static_assert(kStages % 2 == 0 && kLoaders <= kStages, "two scatter groups; loaders may not lap a stage");
+};
+
+// kind::f16 / kind::f8f6f4 instruction descriptor for M = 256 across the pair
+// (FP32 D, A K-major, B N-major, N = 256); E4M3 uses format code 0 as FP16.
+__host__ __device__ constexpr uint32_t idesc_pair()
+{
+    return (1u << 4) | (1u << 16) | ((uint32_t)(kPairN >> 3) << 17) | ((uint32_t)(256 >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_pair_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                              uint32_t accum)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+                 "l"(a), "l"(b), "r"(idesc), "r"(accum)
+                 : "memory");
+}
+__device__ __forceinline__ void umma_pair_f8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                             uint32_t accum)
+{
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "setp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::2.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+                 "l"(a), "l"(b), "r"(idesc), "r"(accum)
+                 : "memory");
+}
+// Arrive on the mbarrier at `bar`'s offset in both CTAs of the pair once every
+// tcgen05.mma this thread issued has completed.
+__device__ __forceinline__ void umma_commit_pair(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+                 ::"r"(smem_u32(bar)), "h"((uint16_t)3)
+                 : "memory");
+}
+
+// Pair work item (job, pair, 256-wide N slice) -> this CTA's two table
+// entries: {A chunk base (-1: empty partner), B chunk base, chunk count,
+// job << 16 | slice} and {window of its rows (-1: none), rotation base, 0, 0}.
+// Both CTAs walk the chunks of the first window's list, so that both load
+// the same B rows for the same chunk.
+__device__ __forceinline__ void decode_pair_item(const TcBatch &batch, int item, uint32_t rank, int4 *e0, int4 *e1)
+{
+    int j = 0;
+    while (j + 1 < batch.n_jobs && batch.item_start[j + 1] <= item) j++;
+    const TcJob &a = batch.job[j];
+    const int local = item - batch.item_start[j];
+    const int2 pr = a.pairs[local / a.ntiles];
+    const int4 w0 = a.win_info[pr.x];
+    const int mine = rank == 0 ? pr.x : pr.y;
+    const int4 wm = mine >= 0 ? a.win_info[mine] : make_int4(-1, -1, 0, 0);
+    *e0 = make_int4(wm.y, w0.y, w0.z, (j << 16) | (local % a.ntiles));
+    *e1 = make_int4(wm.x, w0.x, 0, 0);
+}
+
+template <typename OutT, bool F8>
+__global__ void __launch_bounds__(kThreads, 1) spmm_tc_pair_kernel(const __grid_constant__ TcBatch batch)
+{
+    using Cfg = Tc2Cfg<F8>;
+    constexpr int S = Cfg::kStages;
+    constexpr int kATileBytes = Cfg::kATileBytes;
+    constexpr int kGathers = 16 * Cfg::kBoxes; // gather4 instructions per condensed chunk
+    extern __shared__ __align__(1024) uint8_t smem[];
+    int4 *pend = reinterpret_cast<int4 *>(smem + Cfg::kPendOff);
+    int4 *pend2 = reinterpret_cast<int4 *>(smem + Cfg::kPend2Off);
+    int4 *items = reinterpret_cast<int4 *>(smem + Cfg::kItemOff); // [k][2]
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + Cfg::kBarOff);
+    uint64_t *empty = full + S;
+    uint64_t *staged = empty + S;
+    uint64_t *peer_full = staged + S;    // first CTA: the partner's stage s is full
+    uint64_t *acc_full = peer_full + S;  // [2]
+    uint64_t *acc_empty = acc_full + 2;  // [2], first CTA: both epilogues drained it
+    uint64_t *drain = acc_empty + 2;     // every MMA of the pair has completed
+    uint64_t *bye = drain + 1;           // the partner is done with this CTA's shared memory
+    volatile int *flag = reinterpret_cast<volatile int *>(bye + 1);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bye + 1) + 4;
+    constexpr int kGroupThreads = kScatterThreads / 2;
+
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+
+    const uint32_t rank = cluster_rank();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pair_id = (int)blockIdx.x >> 1, n_pairs_grid = (int)gridDim.x >> 1;
+    const int total = batch.item_start[batch.n_jobs];
+    const int n_items =
+        pair_id < total ? min(kMaxCtaItems, (total - 1 - pair_id) / n_pairs_grid + 1) : 0;
+    // both CTAs are resident before either touches the other's shared memory
+    cluster_sync_all();
+    if (smem_u32(smem) & 1023u) { // the same in both CTAs: both leave here, before any shared state
+        if (threadIdx.x == 0 && n_items > 0)
+            atomicOr(batch.job[0].status, kStatusLayout);
+        return;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(&full[s], kGroupThreads);
+            mbar_init(&empty[s], 1);
+            mbar_init(&staged[s], 1);
+            mbar_init(&peer_full[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 2);
+        }
+        mbar_init(drain, 1);
+        mbar_init(bye, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if ((int)threadIdx.x < n_items)
+        decode_pair_item(batch, pair_id + (int)threadIdx.x * n_pairs_grid, rank, &items[2 * threadIdx.x],
+                         &items[2 * threadIdx.x + 1]);
+    if (warp == kMmaWarp) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(2 * kPairN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    cluster_sync_all(); // barriers initialised and tensor memory allocated in both CTAs
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+    int total_chunks = 0;
+    for (int k = 0; k < n_items; k++) total_chunks += items[2 * k].z;
+
+    if (warp == kLoaderWarp || warp >= kLoaderWarp1) {
+        // ---------------- loaders (as in spmm_tc_kernel; B: this CTA's half of N) ----------------
+        const int ld = warp == kLoaderWarp ? 0 : warp - kLoaderWarp1 + 1;
+        auto advance = [&](int &k, int &i) {
+            while (k < n_items && i >= items[2 * k].z) { i -= items[2 * k].z; k++; }
+        };
+        struct Meta { int4 cols; int img, e0, e1; };
+        auto fetch = [&](int k, int i, Meta &m) {
+            m.cols = make_int4(-1, -1, -1, -1);
+            m.img = -1;
+            m.e0 = m.e1 = 0;
+            if (k < n_items) {
+                const int4 it = items[2 * k], it2 = items[2 * k + 1];
+                const TcJob &a = batch.job[it.w >> 16];
+                const int r = (i + it2.y % it.z) % it.z; // the same chunk order in both CTAs
+                if (lane < 16)
+                    m.cols = __ldg(reinterpret_cast<const int4 *>(a.win_cols + (size_t)(it.y + r) * kChunkCols) + lane);
+                if (it.x >= 0) { // else an empty partner: a zero A tile
+                    m.img = __ldg(a.img_idx + it.x + r);
+                    m.e0 = __ldg(a.tile_ptr + it.x + r);
+                    m.e1 = __ldg(a.tile_ptr + it.x + r + 1);
+                }
+            }
+        };
+        int k = 0, i = ld;
+        advance(k, i);
+        int g = ld;
+        auto step = [&](Meta &cur, Meta &nxt) -> bool {
+            if (g >= total_chunks || !ok)
+                return false;
+            int k2 = k, i2 = i + kLoaders;
+            advance(k2, i2);
+            fetch(k2, i2, nxt);
+            const int s = g % S;
+            uint32_t got = 1;
+            if (lane == 0 && g >= S)
+                got = mbar_poll_cluster(&empty[s], ((g / S) - 1) & 1) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) { ok = false; return false; }
+            const int4 it = items[2 * k];
+            const TcJob &a = batch.job[it.w >> 16];
+            const int n0 = (it.w & 0xffff) * kPairN + (int)rank * Cfg::kHalfCols;
+            const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
+            if (lane == 0) {
+                const int img = cur.img, e0 = cur.e0, e1 = cur.e1, e0a = e0 & ~3;
+                pend[s] = make_int4(img, e0, e0a, e1);
+                pend2[s] = make_int4((i == 0 ? 1 : 0) | (i == it.z - 1 ? 2 : 0), k & 1, k, 0);
+                mbar_expect_tx(&full[s], Cfg::kBTileBytes + (img >= 0 ? kATileBytes : 0));
+                if (img >= 0) {
+                    bulk_copy_g2s(a_s, a.images + (size_t)img * kATileBytes, kATileBytes, &full[s]);
+                    mbar_arrive(&staged[s]);
+                } else if (e1 > e0) {
+                    const uint32_t bytes = (uint32_t)(((e1 - e0a) * 4 + 15) & ~15);
+                    mbar_arrive_expect_tx(&staged[s], bytes);
+                    bulk_copy_g2s(smem_u32(smem + Cfg::kStagingOff + s * kStagingBytes), a.entries + e0a, bytes,
+                                  &staged[s]);
+                } else {
+                    mbar_arrive(&staged[s]);
+                }
+            }
+            __syncwarp();
+            const int col0 = __shfl_sync(0xffffffffu, cur.cols.x, 0);
+            const int col63 = __shfl_sync(0xffffffffu, cur.cols.w, 15);
+            if (col0 >= 0 && col63 == col0 + kChunkCols - 1) {
+                if (lane < Cfg::kBoxes)
+                    tma_tile2d(b_s + lane * (kChunkCols * 128), &a.tmap_tile, n0 + lane * Cfg::kBoxCols, col0,
+                               &full[s]);
+            } else {
+                const int src = lane & 15;
+                const int y0 = __shfl_sync(0xffffffffu, cur.cols.x, src);
+                const int y1 = __shfl_sync(0xffffffffu, cur.cols.y, src);
+                const int y2 = __shfl_sync(0xffffffffu, cur.cols.z, src);
+                const int y3 = __shfl_sync(0xffffffffu, cur.cols.w, src);
+                for (int q = lane; q < kGathers; q += 32) {
+                    const int box = q >> 4;
+                    tma_gather4(b_s + box * (kChunkCols * 128) + src * 512, &a.tmap_b, n0 + box * Cfg::kBoxCols, y0,
+                                y1, y2, y3, &full[s]);
+                }
+            }
+            k = k2;
+            i = i2;
+            g += kLoaders;
+            return true;
+        };
+        Meta ma, mb;
+        fetch(k, i, ma);
+        while (step(ma, mb) && step(mb, ma)) {
+        }
+    } else if (warp < 4) {
+        // ---------------- scatter (as in spmm_tc_kernel, two groups) ----------------
+        const int grp = warp >> 1;
+        const int sid = (int)threadIdx.x - grp * kGroupThreads;
+        int it = 0;
+        for (int g = grp; g < total_chunks; g += 2, it++) {
+            const int s = g % S;
+            volatile int *fl = flag + grp * 2 + (it & 1);
+            if (sid == 0)
+                *fl = mbar_wait(&staged[s], (g / S) & 1) ? 1 : 0;
+            named_bar_sync(1 + grp, kGroupThreads);
+            if (*fl == 0) { ok = false; break; }
+            const int4 pd = pend[s];
+            if (pd.x == -1) {
+                uint8_t *At = smem + s * Cfg::kStage;
+#pragma unroll
+                for (int q = 0; q < kATileBytes / (16 * kGroupThreads); q++)
+                    reinterpret_cast<uint4 *>(At)[sid + q * kGroupThreads] = make_uint4(0, 0, 0, 0);
+                named_bar_sync(1 + grp, kGroupThreads);
+                const uint32_t *st = reinterpret_cast<const uint32_t *>(smem + Cfg::kStagingOff + s * kStagingBytes);
+                for (int e = pd.y + sid; e < pd.w; e += kGroupThreads) {
+                    const uint32_t v = st[e - pd.z];
+                    if constexpr (F8)
+                        At[swz64_offset(v >> 22, (v >> 16) & 63u)] = (uint8_t)(v & 0xffu);
+                    else
+                        *reinterpret_cast<uint16_t *>(At + swz128_offset(v >> 22, (v >> 16) & 63u)) =
+                            (uint16_t)(v & 0xffffu);
+                }
+                fence_proxy_async();
+            }
+            mbar_arrive(&full[s]);
+        }
+    } else if (warp == kMmaWarp) {
+        if (lane == 0) {
+            if (rank == 0) {
+                // ---------------- MMA issuer for the pair ----------------
+                constexpr uint32_t idesc = idesc_pair();
+                const bool withhold = (batch.job[0].flags & TCA_FLAG_TEST_WITHHOLD_ACCUM) != 0;
+                for (int g = 0; g < total_chunks; g++) {
+                    const int s = g % S;
+                    if (!mbar_wait(&full[s], (g / S) & 1) || !mbar_poll_cluster(&peer_full[s], (g / S) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    const int4 f = pend2[s];
+                    const int b = f.y, k = f.z;
+                    if ((f.x & 1) && k >= 2 && !mbar_poll_cluster(&acc_empty[b], ((k >> 1) - 1) & 1)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t a_s = smem_u32(smem + s * Cfg::kStage), b_s = a_s + kATileBytes;
+                    const uint32_t d = tmem + (uint32_t)(b * kPairN);
+                    if constexpr (F8) {
+#pragma unroll
+                        for (int kk = 0; kk < kChunkCols / 32; kk++) {
+                            const uint64_t ad = smem_desc(a_s + kk * 32, 16, 512, 4);
+                            const uint64_t bd = smem_desc(b_s + kk * 4096, kChunkCols * 128, 1024);
+                            umma_pair_f8(d, ad, bd, idesc, ((f.x & 1) && kk == 0) ? 0u : 1u);
+                        }
+                    } else {
+#pragma unroll
+                        for (int kk = 0; kk < kChunkCols / 16; kk++) {
+                            const uint64_t ad = smem_desc(a_s + kk * 32, 16, 1024);
+                            const uint64_t bd = smem_desc(b_s + kk * 2048, kChunkCols * 128, 1024);
+                            umma_pair_f16(d, ad, bd, idesc, ((f.x & 1) && kk == 0) ? 0u : 1u);
+                        }
+                    }
+                    umma_commit_pair(&empty[s]);
+                    if ((f.x & 2) && !(withhold && k == n_items - 1))
+                        umma_commit_pair(&acc_full[b]);
+                }
+                umma_commit_pair(drain);
+            } else {
+                // ---------------- relay: this CTA's stages to the first CTA ----------------
+                for (int g = 0; g < total_chunks; g++) {
+                    const int s = g % S;
+                    if (!mbar_wait(&full[s], (g / S) & 1)) { ok = false; break; }
+                    mbar_arrive_cluster(cluster_map(smem_u32(&peer_full[s]), 0u));
+                }
+            }
+            // every MMA of the pair has completed (both CTAs' tensor memory and
+            // shared memory are no longer read or written by it)
+            if (!mbar_poll_cluster(drain, 0))
+                ok = false;
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue: this CTA's window, all 256 columns ----------------
+        const int quarter = warp & 3;
+        for (int k = 0; k < n_items; k++) {
+            const int4 it = items[2 * k], it2 = items[2 * k + 1];
+            const TcJob &a = batch.job[it.w >> 16];
+            const int n0 = (it.w & 0xffff) * kPairN;
+            const int i = it2.x * kWindowRows + quarter * 32 + lane;
+            int out_row = -1;
+            if (it2.x >= 0 && i < a.M && !((a.flags & TCA_FLAG_KEEP_EMPTY_ROWS) && a.p_row_ptr[i + 1] == a.p_row_ptr[i]))
+                out_row = a.perm[i];
+            const int b = k & 1;
+            if constexpr (F8) {
+                float *sc = reinterpret_cast<float *>(smem + Cfg::kScaleOff) + b * kPairN;
+                for (int c = quarter * 32 + lane; c < kPairN; c += kEpiThreads)
+                    sc[c] = n0 + c < a.N ? __ldg(a.col_scale + n0 + c) : 0.f;
+            }
+            uint32_t got = 0;
+            if (lane == 0)
+                got = mbar_poll_cluster(&acc_full[b], (k >> 1) & 1) ? 1u : 0u;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!named_bar_and(kEpiBar, kEpiThreads, got != 0)) { ok = false; break; }
+            tc_fence_after();
+            OutT *Crow = out_row >= 0 ? reinterpret_cast<OutT *>(a.C) + (size_t)out_row * a.ldc : nullptr;
+            float sa = 1.f;
+            if constexpr (F8)
+                sa = (it2.x >= 0 && i < a.M) ? a.row_scale[i] : 0.f;
+            for (int cb = 0; it2.x >= 0 && cb < kPairN / 16; cb++) {
+                const int n = n0 + cb * 16;
+                if (n >= a.N)
+                    break;
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kPairN + cb * 16), r);
+                if constexpr (F8) {
+                    float *f = reinterpret_cast<float *>(r);
+                    const float *sb = reinterpret_cast<const float *>(smem + Cfg::kScaleOff) + b * kPairN + cb * 16;
+#pragma unroll
+                    for (int q = 0; q < 16; q++) f[q] *= sa * sb[q];
+                }
+                if (Crow) {
+                    store8_out(Crow + n, reinterpret_cast<const float *>(r), a.alpha, a.beta);
+                    if (n + 8 < a.N)
+                        store8_out(Crow + n + 8, reinterpret_cast<const float *>(r) + 8, a.alpha, a.beta);
+                }
+            }
+            tc_fence_before();
+            named_bar_sync(kEpiBar, kEpiThreads); // the four warps are done with buffer b
+            if (warp == kEpiWarp0 && lane == 0) {
+                if (rank == 0)
+                    mbar_arrive(&acc_empty[b]);
+                else
+                    mbar_arrive_cluster(cluster_map(smem_u32(&acc_empty[b]), 0u));
+            }
+        }
+    }
+
+    tc_fence_before();
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) {
+            if (n_items > 0)
+                atomicOr(batch.job[items[0].w >> 16].status, kStatusTimeout);
+            const uint64_t t0 = global_ns();
+            while (global_ns() - t0 < 1000000ull) {
+            }
+        }
+        __syncthreads();
+    }
+    // The partner makes no further access to this CTA's shared memory once
+    // it has arrived here (its roles are done, the MMAs it issued completed);
+    // the wait is bounded like every other.
+    if (threadIdx.x == 0) {
+        mbar_arrive_cluster(cluster_map(smem_u32(bye), rank ^ 1u));
+        if (!mbar_poll_cluster(bye, 0) && n_items > 0)
+            atomicOr(batch.job[items[0].w >> 16].status, kStatusTimeout);
+    }
+    __syncthreads();
+    if (warp == kMmaWarp) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kPairN) : "memory");
+    }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -594,6 +1029,7 @@ int make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT,
         j.col_scale = nullptr;
     }
     j.win_info = p->tc_win_info;
+    j.pairs = p->tc_pairs;
     j.tile_ptr = p->tile_ptr;
     j.win_cols = p->win_cols;
     j.img_idx = p->img_idx;
@@ -644,6 +1080,53 @@ int launch_group_out(const TcBatch &b, int NT, bool f8, cudaStream_t s)
     }
 }
 
+// Pair kernel: clusters of two CTAs (one per SM), persistent over the pair
+// items, as many clusters as fit at once (or more when an item list would
+// exceed kMaxCtaItems per cluster).
+template <typename OutT, bool F8>
+int launch_pair_group(const TcBatch &b, cudaStream_t s)
+{
+    const int smem = Tc2Cfg<F8>::kSmem;
+    auto kernel = spmm_tc_pair_kernel<OutT, F8>;
+    TCA_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    TCA_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    static int max_clusters = 0;
+    if (max_clusters == 0) {
+        cfg.gridDim = dim3(2 * (kSMs / 2));
+        int n = 0;
+        TCA_CUDA_TRY(cudaOccupancyMaxActiveClusters(&n, kernel, &cfg));
+        if (n <= 0)
+            return set_error(TCA_ERR_CUDA, "no CTA pair of the tensor-core pair kernel fits on this device");
+        max_clusters = n;
+    }
+    const int total = b.item_start[b.n_jobs];
+    const int clusters = std::min(total, std::max(max_clusters, (total + kMaxCtaItems - 1) / kMaxCtaItems));
+    cfg.gridDim = dim3((unsigned)(2 * clusters));
+    TCA_CUDA_TRY(cudaLaunchKernelEx(&cfg, kernel, b));
+    return TCA_OK;
+}
+
+int launch_pair_typed(const TcBatch &b, bool f8, int c_dtype, cudaStream_t s)
+{
+    if (b.n_jobs == 0 || b.item_start[b.n_jobs] == 0)
+        return TCA_OK;
+    if (c_dtype == TCA_DTYPE_F16)
+        return f8 ? launch_pair_group<__half, true>(b, s) : launch_pair_group<__half, false>(b, s);
+    return f8 ? launch_pair_group<float, true>(b, s) : launch_pair_group<float, false>(b, s);
+}
+
 int launch_group_typed(const TcBatch &b, int NT, bool f8, int c_dtype, cudaStream_t s)
 {
     if (b.n_jobs == 0 || b.item_start[b.n_jobs] == 0)
@@ -675,10 +1158,12 @@ int tc_block_regs(bool f8, int *regs)
         const void *f16_fns[] = {
             (const void *)spmm_tc_kernel<64, __half, false>, (const void *)spmm_tc_kernel<128, __half, false>,
             (const void *)spmm_tc_kernel<256, __half, false>, (const void *)spmm_tc_kernel<64, float, false>,
-            (const void *)spmm_tc_kernel<128, float, false>, (const void *)spmm_tc_kernel<256, float, false>};
+            (const void *)spmm_tc_kernel<128, float, false>, (const void *)spmm_tc_kernel<256, float, false>,
+            (const void *)spmm_tc_pair_kernel<__half, false>, (const void *)spmm_tc_pair_kernel<float, false>};
         const void *f8_fns[] = {
             (const void *)spmm_tc_kernel<128, __half, true>, (const void *)spmm_tc_kernel<256, __half, true>,
-            (const void *)spmm_tc_kernel<128, float, true>, (const void *)spmm_tc_kernel<256, float, true>};
+            (const void *)spmm_tc_kernel<128, float, true>, (const void *)spmm_tc_kernel<256, float, true>,
+            (const void *)spmm_tc_pair_kernel<__half, true>, (const void *)spmm_tc_pair_kernel<float, true>};
         int w = 0;
         for (const void *f : f16_fns) {
             if (f8) break;
@@ -698,17 +1183,29 @@ int tc_block_regs(bool f8, int *regs)
     return TCA_OK;
 }
 
+// A window alone on a CTA pair keeps two SMs for one window's chunks, so the
+// pair kernel takes a plan when at least two thirds of its tensor-core
+// windows are paired.
+bool pair_eligible(const tca_plan *p, int NT)
+{
+    return NT == kPairN && p->opts.pair_windows != 0 && p->tc_pairs != nullptr && 3 * p->n_full_pairs >= p->n_tc;
+}
+
 int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, float beta, unsigned flags,
                    cudaStream_t s, LaunchList *defer)
 {
-    const int widths[3] = {64, 128, 256};
+    // widths of the single-window kernel, then (0) the pair kernel for N-slices of 256
+    const int widths[4] = {64, 128, 256, 0};
     auto emit = [&](const TcBatch &b, int NT, bool f8) -> int {
         if (b.n_jobs == 0 || b.item_start[b.n_jobs] == 0)
             return TCA_OK;
+        auto run = [NT, f8, c_dtype](const TcBatch &bb, cudaStream_t st) {
+            return NT == 0 ? launch_pair_typed(bb, f8, c_dtype, st) : launch_group_typed(bb, NT, f8, c_dtype, st);
+        };
         if (!defer)
-            return launch_group_typed(b, NT, f8, c_dtype, s);
+            return run(b, s);
         auto held = std::make_shared<TcBatch>(b);
-        defer->push_back([held, NT, f8, c_dtype](cudaStream_t st) { return launch_group_typed(*held, NT, f8, c_dtype, st); });
+        defer->push_back([held, run](cudaStream_t st) { return run(*held, st); });
         return TCA_OK;
     };
     for (bool f8 : {false, true}) {
@@ -718,10 +1215,14 @@ int launch_tc_jobs(const SpmmJob *jobs, int n_jobs, int c_dtype, float alpha, fl
             b.item_start[0] = 0;
             for (int i = 0; i < n_jobs; i++) {
                 const SpmmJob &sj = jobs[i];
-                if (!sj.tc || sj.f8 != f8 || sj.n_tile != NT || sj.p->n_tc == 0 || sj.N <= 0)
+                if (!sj.tc || sj.f8 != f8 || sj.p->n_tc == 0 || sj.N <= 0)
                     continue;
-                TCA_TRY(make_job(sj, alpha, beta, flags, NT, &b.job[b.n_jobs]));
-                b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + sj.p->n_tc * b.job[b.n_jobs].ntiles;
+                const bool pair = pair_eligible(sj.p, sj.n_tile);
+                if (NT == 0 ? !pair : (pair || sj.n_tile != NT))
+                    continue;
+                TCA_TRY(make_job(sj, alpha, beta, flags, NT == 0 ? kPairN : NT, &b.job[b.n_jobs]));
+                const int units = NT == 0 ? sj.p->n_pairs : sj.p->n_tc;
+                b.item_start[b.n_jobs + 1] = b.item_start[b.n_jobs] + units * b.job[b.n_jobs].ntiles;
                 b.n_jobs++;
                 if (b.n_jobs == kMaxJobs) {
                     TCA_TRY(emit(b, NT, f8));

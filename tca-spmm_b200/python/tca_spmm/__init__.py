@@ -31,6 +31,7 @@ ARR_TILE_PTR, ARR_TILE_ENTRIES, ARR_TILE_SRC = 9, 10, 11
 ARR_TILE_IMAGE_IDX, ARR_TILE_IMAGES = 12, 13
 ARR_CC_ITEMS, ARR_ALL_ITEMS = 14, 15
 ARR_ROW_SCALE, ARR_P_VAL_F8, ARR_TILE_ENTRIES_F8, ARR_TILE_IMAGES_F8 = 16, 17, 18, 19
+ARR_TC_PAIRS = 20
 _ARR_DTYPE = {ARR_P_VAL: np.uint16, ARR_TILE_ENTRIES: np.uint32, ARR_TILE_IMAGES: np.uint16,
               ARR_ROW_SCALE: np.float32, ARR_P_VAL_F8: np.uint8, ARR_TILE_ENTRIES_F8: np.uint32,
               ARR_TILE_IMAGES_F8: np.uint8}
@@ -51,7 +52,7 @@ class TcaError(RuntimeError):
 
 class PlanOpts(ctypes.Structure):
     _fields_ = [("sort_rows", ctypes.c_int), ("tc_min_density", ctypes.c_float),
-                ("path", ctypes.c_int), ("reserved", ctypes.c_int * 5)]
+                ("path", ctypes.c_int), ("pair_windows", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
 class PlanInfo(ctypes.Structure):
@@ -229,7 +230,7 @@ class Plan:
     src/our_spmm.cu:347-471)."""
 
     def __init__(self, row_ptr, col_idx, vals, K, sort_rows=True, tc_min_density=None,
-                 path="auto", stream=None):
+                 path="auto", pair_windows=False, stream=None):
         torch = _torch()
         _check_dev("row_ptr", row_ptr, torch.int32)
         _check_dev("col_idx", col_idx, torch.int32)
@@ -241,6 +242,7 @@ class Plan:
         if tc_min_density is not None:
             opts.tc_min_density = float(tc_min_density)
         opts.path = PATHS[path]
+        opts.pair_windows = 1 if pair_windows else 0
         self.M = row_ptr.numel() - 1
         self.K = int(K)
         self.nnz = col_idx.numel()

@@ -92,7 +92,7 @@ PLAN_KEYS = {
     "win_cols": tca_spmm.ARR_WIN_COLS, "tile_ptr": tca_spmm.ARR_TILE_PTR,
     "tile_entries": tca_spmm.ARR_TILE_ENTRIES, "tile_src": tca_spmm.ARR_TILE_SRC,
     "tile_image_idx": tca_spmm.ARR_TILE_IMAGE_IDX, "tile_images": tca_spmm.ARR_TILE_IMAGES,
-    "cc_items": tca_spmm.ARR_CC_ITEMS, "all_items": tca_spmm.ARR_ALL_ITEMS,
+    "cc_items": tca_spmm.ARR_CC_ITEMS, "all_items": tca_spmm.ARR_ALL_ITEMS, "tc_pairs": tca_spmm.ARR_TC_PAIRS,
 }
 
 
