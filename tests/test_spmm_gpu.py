@@ -327,3 +327,35 @@ def test_matches_reference_tca_and_cusparse(cuda, cfg):
     if ref_err < 1e-2:
         assert rel(ours, ref_tca) < 1e-2
     assert our_err < ref_err or our_err < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["f16", "e4m3"])
+def test_batch_of_32_full_size_problems(cuda, precision):
+    """32 sweep problems in one launch (352 tensor-core items on 148
+    persistent CTAs, a third round on 56 of them): the problems of every
+    round against FP64 (E4M3: against the FP64 product of its own quantized
+    operands)."""
+    distinct = [gen.sweep(0.8, N=256, seed=7200 + i) for i in range(4)]
+    plans, Bs, Cs = [], [], []
+    for g in range(32):
+        c = distinct[g % 4]
+        rp, ci, v, B = dev(c, cuda)
+        plans.append(tca_spmm.Plan(rp, ci, v, c["K"]))
+        Bs.append(B)
+        Cs.append(torch.empty((c["M"], 256), dtype=torch.float32, device=cuda))
+    if precision == "f16":
+        tca_spmm.spmm_batched(plans, Bs, Cs)
+    else:
+        tca_spmm.spmm_fp8_batched(plans, Bs, Cs)
+    torch.cuda.synchronize()
+    for p in plans:
+        p.status()
+    if precision == "f16":
+        for g in (0, 27, 29, 30, 31):
+            assert_close(Cs[g], distinct[g % 4])
+    else:
+        refs = [oracle.spmm_fp8_f64(c["row_ptr"], c["col"], c["vals"], c["B"]) for c in distinct]
+        for g in range(32):
+            got = Cs[g].double().cpu().numpy()
+            ref = refs[g % 4]
+            assert np.linalg.norm(got - ref) <= 2e-5 * np.linalg.norm(ref), g
