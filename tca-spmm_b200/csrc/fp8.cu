@@ -61,16 +61,31 @@ __global__ void __launch_bounds__(256)
 k_render_images_f8(const int *__restrict__ img_chunk, const int *__restrict__ tile_ptr,
                    const uint32_t *__restrict__ entries_f8, uint8_t *__restrict__ images)
 {
+    // rendered in shared memory, written out in 16-byte stores (as k_render_images)
+    constexpr int kBytes = kWindowRows * kChunkCols;
+    __shared__ __align__(16) uint8_t tile[kBytes];
     const int m = blockIdx.x;
     const int c = img_chunk[m];
-    uint8_t *img = images + (size_t)m * kWindowRows * kChunkCols;
-    for (int k = threadIdx.x; k < kWindowRows * kChunkCols / 16; k += blockDim.x)
-        reinterpret_cast<uint4 *>(img)[k] = make_uint4(0, 0, 0, 0);
+    for (int k = threadIdx.x; k < kBytes / 16; k += blockDim.x)
+        reinterpret_cast<uint4 *>(tile)[k] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    for (int e = tile_ptr[c] + threadIdx.x; e < tile_ptr[c + 1]; e += blockDim.x) {
-        const uint32_t v = entries_f8[e];
-        img[swz64_offset(v >> 22, (v >> 16) & 63u)] = (uint8_t)(v & 0xffu);
+    const int e0 = tile_ptr[c], e1 = tile_ptr[c + 1];
+    for (int e = e0 + (int)threadIdx.x; e < e1; e += 8 * (int)blockDim.x) { // 8 loads in flight per thread
+        uint32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int eu = e + u * (int)blockDim.x;
+            v[u] = eu < e1 ? entries_f8[eu] : 0xffffffffu;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (v[u] != 0xffffffffu)
+                tile[swz64_offset(v[u] >> 22, (v[u] >> 16) & 63u)] = (uint8_t)(v[u] & 0xffu);
     }
+    __syncthreads();
+    uint4 *img = reinterpret_cast<uint4 *>(images + (size_t)m * kBytes);
+    for (int k = threadIdx.x; k < kBytes / 16; k += blockDim.x)
+        img[k] = reinterpret_cast<const uint4 *>(tile)[k];
 }
 
 // B quantization of up to kMaxQJobs matrices per launch (blockIdx.z = matrix).

@@ -108,7 +108,7 @@ __global__ void k_permute(const int *__restrict__ perm, const int *__restrict__ 
 // stale read costs at most one redundant atomic.
 __device__ __forceinline__ void mark_columns(const int *__restrict__ p_col, int lo, int hi, uint32_t *bm)
 {
-    constexpr int U = 8;
+    constexpr int U = 16; // loads in flight per thread: a window of 128 long rows is ~130K columns
     for (int j0 = lo + threadIdx.x; j0 < hi; j0 += blockDim.x * U) {
         int c[U];
 #pragma unroll
@@ -134,7 +134,7 @@ __device__ __forceinline__ void mark_columns(const int *__restrict__ p_col, int 
 __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
                                const int *__restrict__ p_sorted, int M, int K, const int *__restrict__ err,
                                int *__restrict__ win_nu, int *__restrict__ win_nnz, int *__restrict__ win_elig,
-                               int *__restrict__ win_nblk)
+                               int *__restrict__ win_nblk, uint32_t *__restrict__ bitmaps)
 {
     extern __shared__ uint32_t bm[];
     __shared__ int s_cnt, s_elig, s_nblk;
@@ -151,6 +151,8 @@ __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__r
     for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
         if (!p_sorted[i]) atomicAnd(&s_elig, 0);
     __syncthreads();
+    if (bitmaps) // kept for k_tile_cols, which would otherwise read the window's columns again
+        for (int i = threadIdx.x; i < nwords; i += blockDim.x) bitmaps[(size_t)w * nwords + i] = bm[i];
     int cnt = 0;
     for (int i = threadIdx.x; i < nwords; i += blockDim.x) cnt += __popc(bm[i]);
     atomicAdd(&s_cnt, cnt); // integer sums: order-independent
@@ -197,7 +199,7 @@ __device__ int block_exclusive_scan(int v, int *total, int *scratch)
 // window) and writes its columns, ascending, 64 per chunk, -1 padding.
 __global__ void __launch_bounds__(1024)
 k_tile_cols(const int4 *__restrict__ win_info, const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
-            int M, int K, int *__restrict__ win_cols)
+            int M, int K, const uint32_t *__restrict__ bitmaps, int *__restrict__ win_cols)
 {
     extern __shared__ uint32_t sm[];
     __shared__ int scratch[33];
@@ -209,9 +211,13 @@ k_tile_cols(const int4 *__restrict__ win_info, const int *__restrict__ p_row_ptr
     const int r0 = w * kWindowRows, r1 = min(M, r0 + kWindowRows);
     const int lo = p_row_ptr[r0], hi = p_row_ptr[r1];
 
-    for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
-    __syncthreads();
-    mark_columns(p_col, lo, hi, bm);
+    if (bitmaps) { // the window's column bitmap, as k_window_stats built it
+        for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = bitmaps[(size_t)w * nwords + i];
+    } else {
+        for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
+        __syncthreads();
+        mark_columns(p_col, lo, hi, bm);
+    }
     __syncthreads();
     if (wi.w) { // direct window: every column < K of each touched 64-column block
         for (int b = threadIdx.x; 2 * b < nwords; b += blockDim.x) {
@@ -274,11 +280,12 @@ __device__ __forceinline__ void chunk_row_range(const int4 &wi, int c, int lr, c
     *hi = lower_bound_col(p_col, *lo, min(re, *lo + kChunkCols), next);
 }
 
-// 5b. Nonzeros per chunk: one block of 128 threads (= rows) per chunk.
+// 5b. Nonzeros per chunk: one block of 128 threads (= rows) per chunk; each
+// row's range in the chunk is kept in row_range for 5c.
 __global__ void __launch_bounds__(128)
 k_tile_count(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_info,
              const int *__restrict__ p_row_ptr, const int *__restrict__ p_col, const int *__restrict__ win_cols,
-             int M, int *__restrict__ chunk_nnz)
+             int M, int *__restrict__ chunk_nnz, int2 *__restrict__ row_range)
 {
     __shared__ int scratch[33];
     const int2 cw = chunk_win[blockIdx.x];
@@ -286,6 +293,7 @@ k_tile_count(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_in
     const int *wc = win_cols + (size_t)wi.y * kChunkCols;
     int lo, hi;
     chunk_row_range(wi, cw.y, threadIdx.x, p_row_ptr, p_col, wc, M, &lo, &hi);
+    row_range[(size_t)blockIdx.x * kWindowRows + threadIdx.x] = make_int2(lo, hi);
     int total;
     block_exclusive_scan(hi - lo, &total, scratch);
     if (threadIdx.x == 0)
@@ -294,12 +302,16 @@ k_tile_count(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_in
 
 // 5c. Entries of each chunk, ordered by (row, column): one block per chunk;
 // tile_ptr (the exclusive sum of chunk_nnz) gives the chunk's first entry.
+// Thread = row of the window; a row's columns and values in the chunk are
+// read 8 at a time before any is used (the walk is otherwise one dependent
+// load per entry).
 __global__ void __launch_bounds__(128)
 k_tile_write(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_info,
-             const int *__restrict__ p_row_ptr, const int *__restrict__ p_col, const __half *__restrict__ p_val,
-             const int *__restrict__ win_cols, const int *__restrict__ tile_ptr, int M,
-             uint32_t *__restrict__ entries, int *__restrict__ tile_src)
+             const int *__restrict__ p_col, const __half *__restrict__ p_val, const int *__restrict__ win_cols,
+             const int *__restrict__ tile_ptr, const int2 *__restrict__ row_range, uint32_t *__restrict__ entries,
+             int *__restrict__ tile_src)
 {
+    constexpr int U = 8;
     __shared__ int scratch[33];
     __shared__ int s_cols[kChunkCols];
     const int2 cw = chunk_win[blockIdx.x];
@@ -307,30 +319,40 @@ k_tile_write(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_in
     const int *wc = win_cols + (size_t)wi.y * kChunkCols;
     if (threadIdx.x < kChunkCols)
         s_cols[threadIdx.x] = wc[cw.y * kChunkCols + threadIdx.x];
-    int lo, hi;
-    chunk_row_range(wi, cw.y, threadIdx.x, p_row_ptr, p_col, wc, M, &lo, &hi);
+    const int2 rr = row_range[(size_t)blockIdx.x * kWindowRows + threadIdx.x]; // from k_tile_count
+    const int lo = rr.x, hi = rr.y;
     int total;
     const int off = block_exclusive_scan(hi - lo, &total, scratch); // its barriers also publish s_cols
     const long long base = (long long)tile_ptr[blockIdx.x] + off;
     const int first = s_cols[0];
     const uint32_t lr = threadIdx.x;
-#pragma unroll 4
-    for (int j = lo; j < hi; j++) {
-        const int col = p_col[j];
-        int rk;
-        if (wi.w) {
-            rk = col - first; // direct chunk: 64 consecutive columns
-        } else {             // condensed chunk: position among its ascending columns (-1 padding last)
-            int a = 0, b = kChunkCols;
-            while (a < b) {
-                const int mid = (a + b) >> 1;
-                const int v = s_cols[mid];
-                if (v >= 0 && v < col) a = mid + 1; else b = mid;
-            }
-            rk = a;
+    for (int j0 = lo; j0 < hi; j0 += U) {
+        int col[U];
+        unsigned short val[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            col[u] = j0 + u < hi ? p_col[j0 + u] : 0;
+            val[u] = j0 + u < hi ? __half_as_ushort(p_val[j0 + u]) : (unsigned short)0;
         }
-        entries[base + (j - lo)] = (lr << 22) | ((uint32_t)rk << 16) | (uint32_t)__half_as_ushort(p_val[j]);
-        tile_src[base + (j - lo)] = j;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (j0 + u >= hi)
+                break;
+            int rk;
+            if (wi.w) {
+                rk = col[u] - first; // direct chunk: 64 consecutive columns
+            } else {                 // condensed chunk: position among its ascending columns (-1 padding last)
+                int a = 0, b = kChunkCols;
+                while (a < b) {
+                    const int mid = (a + b) >> 1;
+                    const int v = s_cols[mid];
+                    if (v >= 0 && v < col[u]) a = mid + 1; else b = mid;
+                }
+                rk = a;
+            }
+            entries[base + (j0 + u - lo)] = (lr << 22) | ((uint32_t)rk << 16) | (uint32_t)val[u];
+            tile_src[base + (j0 + u - lo)] = j0 + u;
+        }
     }
 }
 
@@ -349,23 +371,39 @@ __global__ void k_update_entries(const int *__restrict__ tile_src, const __half 
         entries[i] = (entries[i] & 0xffff0000u) | (uint32_t)__half_as_ushort(p_val[tile_src[i]]);
 }
 
-// Dense tile images: one block per image chunk; zero the 128 x 64 tile, then
-// place every entry at its 128-byte-swizzled K-major position (positions are
-// distinct within a chunk, so the result does not depend on thread order).
+// Dense tile images: one block per image chunk renders the 128 x 64 tile in
+// shared memory -- zeroed, then every entry at its 128-byte-swizzled K-major
+// position (positions are distinct within a chunk, so the result does not
+// depend on thread order) -- and writes it out in 16-byte stores.
 __global__ void __launch_bounds__(256)
 k_render_images(const int *__restrict__ img_chunk, const int *__restrict__ tile_ptr,
                 const uint32_t *__restrict__ entries, uint16_t *__restrict__ images)
 {
+    constexpr int kBytes = kWindowRows * kChunkCols * 2;
+    __shared__ __align__(16) uint8_t tile[kBytes];
     const int m = blockIdx.x;
     const int c = img_chunk[m];
-    uint8_t *img = reinterpret_cast<uint8_t *>(images + (size_t)m * kWindowRows * kChunkCols);
-    for (int k = threadIdx.x; k < kWindowRows * kChunkCols * 2 / 16; k += blockDim.x)
-        reinterpret_cast<uint4 *>(img)[k] = make_uint4(0, 0, 0, 0);
+    for (int k = threadIdx.x; k < kBytes / 16; k += blockDim.x)
+        reinterpret_cast<uint4 *>(tile)[k] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    for (int e = tile_ptr[c] + threadIdx.x; e < tile_ptr[c + 1]; e += blockDim.x) {
-        const uint32_t v = entries[e];
-        *reinterpret_cast<uint16_t *>(img + swz128_offset(v >> 22, (v >> 16) & 63u)) = (uint16_t)(v & 0xffffu);
+    const int e0 = tile_ptr[c], e1 = tile_ptr[c + 1];
+    for (int e = e0 + (int)threadIdx.x; e < e1; e += 8 * (int)blockDim.x) { // 8 loads in flight per thread
+        uint32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int eu = e + u * (int)blockDim.x;
+            v[u] = eu < e1 ? entries[eu] : 0xffffffffu;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (v[u] != 0xffffffffu)
+                *reinterpret_cast<uint16_t *>(tile + swz128_offset(v[u] >> 22, (v[u] >> 16) & 63u)) =
+                    (uint16_t)(v[u] & 0xffffu);
     }
+    __syncthreads();
+    uint4 *img = reinterpret_cast<uint4 *>(images + (size_t)m * kWindowRows * kChunkCols);
+    for (int k = threadIdx.x; k < kBytes / 16; k += blockDim.x)
+        img[k] = reinterpret_cast<const uint4 *>(tile)[k];
 }
 
 unsigned blocks_for(long long n, int per) { return (unsigned)((n + per - 1) / per); }
@@ -521,10 +559,19 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     TCA_TRY(dev_alloc(&d_stage, n_stage, nullptr)); t_stage.p = d_stage;
     int *d_nu = d_stage, *d_wn = d_stage + W, *d_el = d_stage + 2 * W, *d_nb = d_stage + 3 * W;
     const bool tc_possible = (p->opts.path != 1) && K <= kMaxTcK && K > 0 && W > 0;
+    // the windows' column bitmaps, kept from the statistics for the tile
+    // columns when they take at most 64 MB (else k_tile_cols rebuilds them)
+    DevBuf t_bm;
+    uint32_t *d_bm = nullptr;
+    if (tc_possible && (size_t)W * ((K + 31) / 32) <= (size_t)(16u << 20)) {
+        TCA_TRY(dev_alloc(&d_bm, (size_t)W * ((K + 31) / 32), nullptr));
+        t_bm.p = d_bm;
+    }
     if (tc_possible) {
         const size_t smem = sizeof(uint32_t) * ((K + 31) / 32);
         TCA_CUDA_TRY(cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_window_stats<<<W, 1024, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, err, d_nu, d_wn, d_el, d_nb);
+        k_window_stats<<<W, 1024, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, err, d_nu, d_wn, d_el, d_nb,
+                                             d_bm);
         TCA_CUDA_TRY(cudaGetLastError());
     } else if (W > 0) {
         TCA_CUDA_TRY(cudaMemsetAsync(d_stage, 0, sizeof(int) * 4 * (size_t)W, s));
@@ -622,25 +669,26 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         h_cw.reserve((size_t)p->n_tc_chunks);
         for (int t = 0; t < p->n_tc; t++)
             for (int c = 0; c < h_wi[t].z; c++) h_cw.push_back(make_int2(t, c));
-        DevBuf t_cw, t_cn, t_scan;
-        int2 *d_cw;
+        DevBuf t_cw, t_cn, t_scan, t_rr;
+        int2 *d_cw, *d_rr;
         int *d_cn;
         TCA_TRY(dev_alloc(&d_cw, (size_t)p->n_tc_chunks, nullptr)); t_cw.p = d_cw;
         TCA_TRY(dev_alloc(&d_cn, (size_t)p->n_tc_chunks + 1, nullptr)); t_cn.p = d_cn;
+        TCA_TRY(dev_alloc(&d_rr, (size_t)p->n_tc_chunks * kWindowRows, nullptr)); t_rr.p = d_rr;
         TCA_CUDA_TRY(cudaMemcpyAsync(d_cw, h_cw.data(), sizeof(int2) * h_cw.size(), cudaMemcpyHostToDevice, s));
         TCA_CUDA_TRY(cudaMemsetAsync(d_cn + p->n_tc_chunks, 0, sizeof(int), s));
         const size_t smem = 2 * sizeof(uint32_t) * ((K + 31) / 32);
         TCA_CUDA_TRY(cudaFuncSetAttribute(k_tile_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tile_cols<<<p->n_tc, 1024, smem, s>>>(p->tc_win_info, p->p_row_ptr, p->p_col, M, K, p->win_cols);
+        k_tile_cols<<<p->n_tc, 1024, smem, s>>>(p->tc_win_info, p->p_row_ptr, p->p_col, M, K, d_bm, p->win_cols);
         k_tile_count<<<p->n_tc_chunks, 128, 0, s>>>(d_cw, p->tc_win_info, p->p_row_ptr, p->p_col, p->win_cols, M,
-                                                    d_cn);
+                                                    d_cn, d_rr);
         size_t tmp = 0;
         TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_cn, p->tile_ptr, p->n_tc_chunks + 1, s));
         void *tb;
         TCA_TRY(dev_alloc((char **)&tb, tmp, nullptr)); t_scan.p = tb;
         TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tb, tmp, d_cn, p->tile_ptr, p->n_tc_chunks + 1, s));
-        k_tile_write<<<p->n_tc_chunks, 128, 0, s>>>(d_cw, p->tc_win_info, p->p_row_ptr, p->p_col, p->p_val,
-                                                    p->win_cols, p->tile_ptr, M, p->tile_entries, p->tile_src);
+        k_tile_write<<<p->n_tc_chunks, 128, 0, s>>>(d_cw, p->tc_win_info, p->p_col, p->p_val, p->win_cols,
+                                                    p->tile_ptr, d_rr, p->tile_entries, p->tile_src);
         TCA_CUDA_TRY(cudaGetLastError());
     } else {
         TCA_CUDA_TRY(cudaMemsetAsync(p->tile_ptr, 0, sizeof(int), s));
