@@ -718,19 +718,21 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     }
 
     // 7. CUDA-core work items. The host arrays copied to the device here (and
-    // above) may be reused or freed as soon as the copy call returns: a copy
-    // from pageable host memory returns once the data is staged.
-    std::vector<int2> items;
-    build_items(cc_list, h_rp, M, items);
-    p->n_cc_items = (int)items.size();
-    TCA_TRY(dev_alloc(&p->cc_items, items.size(), bytes));
-    if (!items.empty())
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->cc_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
-    build_items(h_all, h_rp, M, items);
-    p->n_all_items = (int)items.size();
-    TCA_TRY(dev_alloc(&p->all_items, items.size(), bytes));
-    if (!items.empty())
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->all_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
+    // above) are pageable, so a copy returns once its data is staged; each
+    // copy still has a source array of its own.
+    std::vector<int2> cc_items, all_items;
+    build_items(cc_list, h_rp, M, cc_items);
+    p->n_cc_items = (int)cc_items.size();
+    TCA_TRY(dev_alloc(&p->cc_items, cc_items.size(), bytes));
+    if (!cc_items.empty())
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->cc_items, cc_items.data(), sizeof(int2) * cc_items.size(),
+                                     cudaMemcpyHostToDevice, s));
+    build_items(h_all, h_rp, M, all_items);
+    p->n_all_items = (int)all_items.size();
+    TCA_TRY(dev_alloc(&p->all_items, all_items.size(), bytes));
+    if (!all_items.empty())
+        TCA_CUDA_TRY(cudaMemcpyAsync(p->all_items, all_items.data(), sizeof(int2) * all_items.size(),
+                                     cudaMemcpyHostToDevice, s));
     if (sync_end)
         TCA_CUDA_TRY(cudaStreamSynchronize(s)); // the plan is complete, for work on any stream
     return TCA_OK;
