@@ -161,7 +161,7 @@ namespace {
 struct HostPath {
     int dev = -1;
     cudaStream_t s = nullptr, s2 = nullptr;
-    cudaEvent_t ready = nullptr, e0 = nullptr, e1 = nullptr;
+    cudaEvent_t ready = nullptr, cols_in = nullptr, e0 = nullptr, e1 = nullptr;
 };
 int host_path(HostPath **out)
 {
@@ -178,6 +178,7 @@ int host_path(HostPath **out)
     TCA_CUDA_TRY(cudaStreamCreateWithFlags(&h.s, cudaStreamNonBlocking));
     TCA_CUDA_TRY(cudaStreamCreateWithFlags(&h.s2, cudaStreamNonBlocking));
     TCA_CUDA_TRY(cudaEventCreateWithFlags(&h.ready, cudaEventDisableTiming));
+    TCA_CUDA_TRY(cudaEventCreateWithFlags(&h.cols_in, cudaEventDisableTiming));
     TCA_CUDA_TRY(cudaEventCreate(&h.e0));
     TCA_CUDA_TRY(cudaEventCreate(&h.e1));
     paths.push_back(h);
@@ -214,7 +215,7 @@ int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals
     const size_t c_elem = (c_dtype == TCA_DTYPE_F16) ? 2 : 4;
     int *d_rp = nullptr, *d_ci = nullptr;
     __half *d_v = nullptr, *d_B = nullptr;
-    void *d_C = nullptr;
+    void *d_C = nullptr, *d_all = nullptr;
     tca_plan_t plan = nullptr;
     int st = TCA_OK;
     auto fail_cuda = [&](cudaError_t e, const char *what) {
@@ -222,19 +223,25 @@ int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals
     };
     do {
         cudaError_t e;
-        if ((st = dev_malloc((void **)&d_rp, sizeof(int) * (size_t)(M + 1), s)) != TCA_OK) break;
-        if ((st = dev_malloc((void **)&d_ci, sizeof(int) * (size_t)(nnz > 0 ? nnz : 1), s)) != TCA_OK) break;
-        if ((st = dev_malloc((void **)&d_v, 2 * (size_t)(nnz > 0 ? nnz : 1), s)) != TCA_OK) break;
-        if ((st = dev_malloc((void **)&d_B, 2 * (size_t)(K > 0 ? K : 1) * N, s)) != TCA_OK) break;
-        if ((st = dev_malloc(&d_C, c_elem * (size_t)M * N, s)) != TCA_OK) break;
-        // the allocations are ordered on s; the second stream's copies come after them
-        if ((e = cudaEventRecord(hp->ready, s)) != cudaSuccess) { fail_cuda(e, "cudaEventRecord"); break; }
-        if ((e = cudaStreamWaitEvent(s2, hp->ready, 0)) != cudaSuccess) { fail_cuda(e, "cudaStreamWaitEvent"); break; }
+        // the five device buffers in one allocation, each at a 256-byte boundary
+        auto span = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        const size_t b_rp = span(sizeof(int) * (size_t)(M + 1)), b_ci = span(sizeof(int) * (size_t)nnz),
+                     b_v = span(2 * (size_t)nnz), b_B = span(2 * (size_t)K * N), b_C = span(c_elem * (size_t)M * N);
+        if ((st = dev_malloc(&d_all, b_rp + b_ci + b_v + b_B + b_C, s)) != TCA_OK) break;
+        char *base = static_cast<char *>(d_all);
+        d_rp = reinterpret_cast<int *>(base);
+        d_ci = reinterpret_cast<int *>(base + b_rp);
+        d_v = reinterpret_cast<__half *>(base + b_rp + b_ci);
+        d_B = reinterpret_cast<__half *>(base + b_rp + b_ci + b_v);
+        d_C = base + b_rp + b_ci + b_v + b_B;
+        // the row offsets and columns first (the plan build starts on them),
+        // then, on the second stream, the values, B and C: the first copies
+        // have the link to themselves
         if ((e = cudaMemcpyAsync(d_rp, h_row_ptr, sizeof(int) * (size_t)(M + 1), cudaMemcpyHostToDevice, s)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
-        if (nnz > 0) {
-            if ((e = cudaMemcpyAsync(d_ci, h_col_idx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
-            if ((e = cudaMemcpyAsync(d_v, h_vals_f16, 2 * (size_t)nnz, cudaMemcpyHostToDevice, s2)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
-        }
+        if (nnz > 0 && (e = cudaMemcpyAsync(d_ci, h_col_idx, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
+        if ((e = cudaEventRecord(hp->cols_in, s)) != cudaSuccess) { fail_cuda(e, "cudaEventRecord"); break; }
+        if ((e = cudaStreamWaitEvent(s2, hp->cols_in, 0)) != cudaSuccess) { fail_cuda(e, "cudaStreamWaitEvent"); break; }
+        if (nnz > 0 && (e = cudaMemcpyAsync(d_v, h_vals_f16, 2 * (size_t)nnz, cudaMemcpyHostToDevice, s2)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
         if (K > 0 && (e = cudaMemcpyAsync(d_B, h_B_f16, 2 * (size_t)K * N, cudaMemcpyHostToDevice, s2)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
         if (flags & TCA_FLAG_KEEP_EMPTY_ROWS) {
             if ((e = cudaMemcpyAsync(d_C, h_C, c_elem * (size_t)M * N, cudaMemcpyHostToDevice, s2)) != cudaSuccess) { fail_cuda(e, "cudaMemcpy"); break; }
@@ -264,8 +271,7 @@ int tca_spmm_host(const int *h_row_ptr, const int *h_col_idx, const void *h_vals
         cudaStreamSynchronize(s);
     }
     if (plan) tca_plan_destroy(plan);
-    for (void *ptr : {(void *)d_rp, (void *)d_ci, (void *)d_v, (void *)d_B, d_C})
-        if (ptr) dev_free(ptr, s);
+    if (d_all) dev_free(d_all, s);
     return st;
 }
 

@@ -24,6 +24,7 @@
 //   6. dense 16 KB images of the chunks with >= 512 entries; CUDA-core
 //      work items (host).
 #include <cub/cub.cuh>
+#include <cstring>
 #include <vector>
 #include <algorithm>
 #include "tca_internal.cuh"
@@ -35,11 +36,19 @@ namespace {
 constexpr int kErrRowPtr = 1, kErrColRange = 2;
 
 // 1. Row checks: one warp per row.
+// Also fills all_windows (window w at index w) and clears the plan's status
+// word.
 __global__ void k_row_check(const int *__restrict__ row_ptr, const int *__restrict__ col, int M, int K, int nnz,
-                            int *__restrict__ row_nnz, int *__restrict__ row_sorted, int *__restrict__ err)
+                            int *__restrict__ row_nnz, int *__restrict__ row_sorted, int *__restrict__ err,
+                            int *__restrict__ all_windows, int W, int *__restrict__ status)
 {
     const int lane = threadIdx.x & 31;
-    const long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < W)
+        all_windows[g] = (int)g;
+    if (g == 0)
+        *status = 0;
+    const long long r = g >> 5;
     if (r >= M)
         return;
     const int s = row_ptr[r], e = row_ptr[r + 1];
@@ -68,11 +77,137 @@ __global__ void k_row_check(const int *__restrict__ row_ptr, const int *__restri
     }
 }
 
+// 2. Row order of a matrix with at most kOrderRows rows, in one block: a
+// stable descending radix sort of the row lengths (ties keep row order; only
+// the bits up to the longest row take part) carrying (row << 1 | sorted
+// flag), the exclusive prefix sum of the sorted lengths (the sorted row
+// offsets), and copies of the offsets and of the check verdict into the
+// array the host reads after step 3. Global loads and stores are striped
+// (coalesced), exchanged through shared memory with the sort's blocked order.
+constexpr int kOrderThreads = 1024, kOrderItems = 8, kOrderRows = kOrderThreads * kOrderItems;
+
+__global__ void __launch_bounds__(kOrderThreads)
+k_order_small(const int *__restrict__ row_nnz, const int *__restrict__ row_sorted, int M, int sort,
+              const int *__restrict__ err, int *__restrict__ perm, int *__restrict__ p_row_ptr,
+              int *__restrict__ p_sorted, int *__restrict__ stage_err, int *__restrict__ stage_rp)
+{
+    using Sort = cub::BlockRadixSort<unsigned, kOrderThreads, kOrderItems, unsigned>;
+    using Scan = cub::BlockScan<int, kOrderThreads>;
+    using Xchg = cub::BlockExchange<unsigned, kOrderThreads, kOrderItems>;
+    __shared__ union {
+        typename Sort::TempStorage sort;
+        typename Scan::TempStorage scan;
+        typename Xchg::TempStorage xchg;
+    } tmp;
+    __shared__ unsigned longest;
+    const int t = threadIdx.x;
+    if (t == 0)
+        longest = 0;
+    unsigned key[kOrderItems], val[kOrderItems], mx = 0;
+#pragma unroll
+    for (int u = 0; u < kOrderItems; u++) { // striped: item u of thread t is row u * 1024 + t
+        const int i = u * kOrderThreads + t;
+        key[u] = i < M ? (unsigned)row_nnz[i] : 0u; // lengths are >= 0; padding sorts after the rows
+        val[u] = i < M ? (unsigned)row_sorted[i] : 0u;
+        mx = max(mx, key[u]);
+    }
+    __syncthreads(); // longest
+    Xchg(tmp.xchg).StripedToBlocked(key, key);
+    __syncthreads();
+    Xchg(tmp.xchg).StripedToBlocked(val, val);
+#pragma unroll
+    for (int u = 0; u < kOrderItems; u++) // blocked: item u of thread t is row t * 8 + u
+        val[u] = ((unsigned)(t * kOrderItems + u) << 1) | (val[u] & 1u);
+    if (sort) {
+        mx = __reduce_max_sync(0xffffffffu, mx);
+        if ((t & 31) == 0)
+            atomicMax(&longest, mx);
+        __syncthreads();
+        const int end_bit = longest ? 32 - __clz((int)longest) : 1;
+        Sort(tmp.sort).SortDescending(key, val, 0, end_bit);
+    }
+    __syncthreads();
+    int len[kOrderItems], off[kOrderItems], total;
+#pragma unroll
+    for (int u = 0; u < kOrderItems; u++)
+        len[u] = (int)key[u];
+    Scan(tmp.scan).ExclusiveSum(len, off, total);
+    unsigned offs[kOrderItems];
+#pragma unroll
+    for (int u = 0; u < kOrderItems; u++)
+        offs[u] = (unsigned)off[u];
+    __syncthreads();
+    Xchg(tmp.xchg).BlockedToStriped(offs, offs);
+    __syncthreads();
+    Xchg(tmp.xchg).BlockedToStriped(val, val);
+#pragma unroll
+    for (int u = 0; u < kOrderItems; u++) {
+        const int i = u * kOrderThreads + t;
+        if (i < M) {
+            perm[i] = (int)(val[u] >> 1);
+            p_sorted[i] = (int)(val[u] & 1u);
+            p_row_ptr[i] = (int)offs[u];
+            stage_rp[i] = (int)offs[u];
+        }
+    }
+    if (t == 0) {
+        p_row_ptr[M] = total;
+        stage_rp[M] = total;
+        *stage_err = *err;
+    }
+}
+
+// Exclusive prefix sum of n values into out[0, n] (out[n] = the total), in
+// one block: the tile offsets of up to kScanSmallMax chunks.
+constexpr int kScanThreads = 1024, kScanItems = 8, kScanSmallMax = 8 * kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_small(const int *__restrict__ in, int n, int *__restrict__ out)
+{
+    using Scan = cub::BlockScan<int, kScanThreads>;
+    __shared__ typename Scan::TempStorage tmp;
+    int carry = 0;
+    for (int base = 0; base < n; base += kScanThreads * kScanItems) {
+        int v[kScanItems], o[kScanItems], agg;
+#pragma unroll
+        for (int u = 0; u < kScanItems; u++) {
+            const int i = base + (int)threadIdx.x * kScanItems + u;
+            v[u] = i < n ? in[i] : 0;
+        }
+        Scan(tmp).ExclusiveSum(v, o, agg);
+#pragma unroll
+        for (int u = 0; u < kScanItems; u++) {
+            const int i = base + (int)threadIdx.x * kScanItems + u;
+            if (i < n)
+                out[i] = carry + o[u];
+        }
+        carry += agg;
+        __syncthreads(); // tmp is reused by the next tile
+    }
+    if (threadIdx.x == 0)
+        out[n] = carry;
+}
+
 __global__ void k_iota(int *a, int n)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         a[i] = (int)i;
+}
+
+// Clears and copies of the build's own arrays are kernels: a memset or a
+// device-to-device copy may run on a copy engine, queued behind the
+// host-to-device copies of the values and B on the host-buffer path's second
+// stream, which steps 1-5 do not wait for.
+__global__ void k_zero_words(uint32_t *__restrict__ p, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = 0u;
+}
+
+__global__ void k_copy_words(const int *__restrict__ src, int *__restrict__ dst, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
 }
 
 __global__ void k_gather_int(const int *__restrict__ src, const int *__restrict__ idx, int *__restrict__ dst, int n)
@@ -83,7 +218,8 @@ __global__ void k_gather_int(const int *__restrict__ src, const int *__restrict_
 }
 
 // 2b. Re-order the CSR: one warp per sorted row. Does nothing when the row
-// checks found an error (the host reports it after its next wait).
+// checks found an error (the host reports it after its next wait). With val
+// NULL the values are left for k_update_p_val (gathered through src).
 __global__ void k_permute(const int *__restrict__ perm, const int *__restrict__ row_ptr,
                           const int *__restrict__ col, const __half *__restrict__ val,
                           const int *__restrict__ p_row_ptr, int M, const int *__restrict__ err,
@@ -97,7 +233,8 @@ __global__ void k_permute(const int *__restrict__ perm, const int *__restrict__ 
     const int s = row_ptr[r], e = row_ptr[r + 1], d = p_row_ptr[i];
     for (int j = lane; j < e - s; j += 32) {
         p_col[d + j] = col[s + j];
-        p_val[d + j] = val[s + j];
+        if (val)
+            p_val[d + j] = val[s + j];
         src[d + j] = s + j;
     }
 }
@@ -129,8 +266,64 @@ __device__ __forceinline__ void mark_columns(const int *__restrict__ p_col, int 
     }
 }
 
-// 3. Window statistics: one block per window, K-bit bitmap in shared memory.
-// Does nothing when the row checks found an error (see k_permute).
+// 3. Window statistics with each window's nonzeros split over `split`
+// blocks, so that a few windows still spread over the GPU: a block marks its
+// share of the columns in a shared-memory bitmap and ORs the set words into
+// the window's global bitmap (zeroed beforehand, kept for k_tile_cols); the
+// window's last block to finish (a per-window counter, zeroed beforehand)
+// counts the distinct columns and touched 64-column blocks from it and
+// checks the rows' flags. Does nothing when the row checks found an error.
+__global__ void __launch_bounds__(512)
+k_window_stats_split(const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
+                     const int *__restrict__ p_sorted, int M, int K, const int *__restrict__ err, int split,
+                     int *__restrict__ win_nu, int *__restrict__ win_nnz, int *__restrict__ win_elig,
+                     int *__restrict__ win_nblk, uint32_t *__restrict__ bitmaps, int *__restrict__ done)
+{
+    extern __shared__ uint32_t bm[];
+    __shared__ int s_cnt, s_elig, s_nblk, s_last;
+    const int w = blockIdx.x / split, part = blockIdx.x % split;
+    if (*err)
+        return; // uniform across the grid
+    const int nwords = (K + 31) >> 5;
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x) bm[i] = 0u;
+    if (threadIdx.x == 0) { s_cnt = 0; s_elig = 1; s_nblk = 0; }
+    __syncthreads();
+    const int r0 = w * kWindowRows, r1 = min(M, r0 + kWindowRows);
+    const int lo = p_row_ptr[r0], hi = p_row_ptr[r1];
+    const int a = lo + (int)((long long)(hi - lo) * part / split);
+    const int b = lo + (int)((long long)(hi - lo) * (part + 1) / split);
+    mark_columns(p_col, a, b, bm);
+    __syncthreads();
+    uint32_t *gbm = bitmaps + (size_t)w * nwords;
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x)
+        if (bm[i]) atomicOr(&gbm[i], bm[i]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+        s_last = atomicAdd(&done[w], 1) == split - 1;
+    __syncthreads();
+    if (!s_last)
+        return;
+    __threadfence(); // the other blocks' words are visible to the last one
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+        if (!p_sorted[i]) atomicAnd(&s_elig, 0);
+    int cnt = 0, nb = 0;
+    for (int i = threadIdx.x; i < nwords; i += blockDim.x) cnt += __popc(__ldcg(gbm + i));
+    for (int q = threadIdx.x; 2 * q < nwords; q += blockDim.x)
+        nb += ((__ldcg(gbm + 2 * q) | (2 * q + 1 < nwords ? __ldcg(gbm + 2 * q + 1) : 0u)) != 0u);
+    atomicAdd(&s_cnt, cnt); // integer sums: order-independent
+    atomicAdd(&s_nblk, nb);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        win_nu[w] = s_cnt;
+        win_nnz[w] = hi - lo;
+        win_elig[w] = s_elig;
+        win_nblk[w] = s_nblk;
+    }
+}
+
+// 3 (bitmaps too large to keep). One block per window, K-bit bitmap in
+// shared memory. Does nothing when the row checks found an error.
 __global__ void k_window_stats(const int *__restrict__ p_row_ptr, const int *__restrict__ p_col,
                                const int *__restrict__ p_sorted, int M, int K, const int *__restrict__ err,
                                int *__restrict__ win_nu, int *__restrict__ win_nnz, int *__restrict__ win_elig,
@@ -252,107 +445,129 @@ k_tile_cols(const int4 *__restrict__ win_info, const int *__restrict__ p_row_ptr
     for (int k = nu + threadIdx.x; k < nch * kChunkCols; k += blockDim.x) wc[k] = -1;
 }
 
-// First position in the sorted columns p_col[a, b) whose column is >= v.
-__device__ __forceinline__ int lower_bound_col(const int *__restrict__ p_col, int a, int b, int v)
+// The nonzeros of local row lr of chunk c of a window are the row's columns
+// from the chunk's first column up to the next chunk's first (a chunk holds
+// at most 64 columns of a row). First index j in [rs, re) with p_col[j] >= x,
+// for a row whose columns increase strictly, by a warp: rounds of 32 samples (the last column of each
+// of 32 equal segments) narrow the range to one segment, whose at most 32
+// columns one warp-wide load then counts. A row of up to 1024 columns takes
+// two dependent loads per lane instead of ~10.
+__device__ __forceinline__ int warp_lower_bound(const int *__restrict__ p_col, int rs, int re, int x, int lane)
 {
-    while (a < b) {
-        const int mid = (a + b) >> 1;
-        if (p_col[mid] < v) a = mid + 1; else b = mid;
+    int a = rs, n = re - rs;
+    while (n > 32) {
+        const int seg = (n + 31) >> 5;
+        const int j = a + min(n, (lane + 1) * seg) - 1; // last column of segment `lane` (or of the row)
+        const int k = __popc(__ballot_sync(0xffffffffu, p_col[j] < x)); // segments wholly below x
+        if (k * seg >= n)
+            return re;
+        a += k * seg;
+        n = min(seg, n - k * seg);
     }
-    return a;
+    return a + __popc(__ballot_sync(0xffffffffu, lane < n && p_col[a + lane] < x));
 }
 
-// The nonzeros of local row lr of chunk c of window wi are p_col[*lo, *hi):
-// the row's columns from the chunk's first column up to the next chunk's
-// first column (a chunk holds at most 64 columns of a row).
-__device__ __forceinline__ void chunk_row_range(const int4 &wi, int c, int lr, const int *__restrict__ p_row_ptr,
-                                                const int *__restrict__ p_col, const int *__restrict__ wc, int M,
-                                                int *lo, int *hi)
-{
-    const int i = wi.x * kWindowRows + lr;
-    *lo = *hi = 0;
-    if (i >= M)
-        return;
-    const int rs = p_row_ptr[i], re = p_row_ptr[i + 1];
-    const int first = wc[c * kChunkCols];
-    const int next = c + 1 < wi.z ? wc[(c + 1) * kChunkCols] : 0x7fffffff;
-    *lo = lower_bound_col(p_col, rs, re, first);
-    *hi = lower_bound_col(p_col, *lo, min(re, *lo + kChunkCols), next);
-}
+// Tile count and tile write: 4 blocks of 32 warps per chunk, a warp per row.
+constexpr int kTileBlocksPerChunk = kWindowRows / 32;
 
-// 5b. Nonzeros per chunk: one block of 128 threads (= rows) per chunk; each
-// row's range in the chunk is kept in row_range for 5c.
-__global__ void __launch_bounds__(128)
+// 5b. Nonzeros per chunk. A row's range in the chunk: its first column at or
+// after the chunk's first (warp_lower_bound), its end among the next 64
+// entries (64 columns, strictly increasing) by one warp-wide count. The range
+// goes to row_range for 5c, its length (summed per block) to chunk_nnz,
+// which is zeroed beforehand.
+__global__ void __launch_bounds__(1024)
 k_tile_count(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_info,
              const int *__restrict__ p_row_ptr, const int *__restrict__ p_col, const int *__restrict__ win_cols,
              int M, int *__restrict__ chunk_nnz, int2 *__restrict__ row_range)
 {
-    __shared__ int scratch[33];
-    const int2 cw = chunk_win[blockIdx.x];
+    __shared__ int s_sum;
+    const int chunk = blockIdx.x / kTileBlocksPerChunk;
+    const int lane = threadIdx.x & 31, lr = (blockIdx.x % kTileBlocksPerChunk) * 32 + (threadIdx.x >> 5);
+    if (threadIdx.x == 0)
+        s_sum = 0;
+    __syncthreads();
+    const int2 cw = chunk_win[chunk];
     const int4 wi = win_info[cw.x];
     const int *wc = win_cols + (size_t)wi.y * kChunkCols;
-    int lo, hi;
-    chunk_row_range(wi, cw.y, threadIdx.x, p_row_ptr, p_col, wc, M, &lo, &hi);
-    row_range[(size_t)blockIdx.x * kWindowRows + threadIdx.x] = make_int2(lo, hi);
-    int total;
-    block_exclusive_scan(hi - lo, &total, scratch);
-    if (threadIdx.x == 0)
-        chunk_nnz[blockIdx.x] = total;
+    const int i = wi.x * kWindowRows + lr;
+    int lo = 0, hi = 0;
+    if (i < M) { // uniform across the warp
+        const int rs = p_row_ptr[i], re = p_row_ptr[i + 1];
+        const int first = wc[cw.y * kChunkCols];
+        const int next = cw.y + 1 < wi.z ? wc[(cw.y + 1) * kChunkCols] : 0x7fffffff;
+        lo = warp_lower_bound(p_col, rs, re, first, lane);
+        const int e = min(re, lo + kChunkCols);
+        const int j0 = lo + lane, j1 = lo + 32 + lane;
+        const bool in0 = j0 < e && p_col[j0] < next, in1 = j1 < e && p_col[j1] < next;
+        hi = lo + __popc(__ballot_sync(0xffffffffu, in0)) + __popc(__ballot_sync(0xffffffffu, in1));
+    }
+    if (lane == 0) {
+        row_range[(size_t)chunk * kWindowRows + lr] = make_int2(lo, hi);
+        if (hi > lo)
+            atomicAdd(&s_sum, hi - lo);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_sum > 0)
+        atomicAdd(&chunk_nnz[chunk], s_sum); // integer sums: order-independent
 }
 
-// 5c. Entries of each chunk, ordered by (row, column): one block per chunk;
-// tile_ptr (the exclusive sum of chunk_nnz) gives the chunk's first entry.
-// Thread = row of the window; a row's columns and values in the chunk are
-// read 8 at a time before any is used (the walk is otherwise one dependent
-// load per entry).
-__global__ void __launch_bounds__(128)
+// 5c. Entries of each chunk, ordered by (row, column): a warp per row writes
+// the row's (at most 64) entries with coalesced loads and stores. Each block
+// scans the chunk's 128 row lengths for the rows' first entries; tile_ptr
+// (the exclusive sum of chunk_nnz) gives the chunk's.
+__global__ void __launch_bounds__(1024)
 k_tile_write(const int2 *__restrict__ chunk_win, const int4 *__restrict__ win_info,
              const int *__restrict__ p_col, const __half *__restrict__ p_val, const int *__restrict__ win_cols,
              const int *__restrict__ tile_ptr, const int2 *__restrict__ row_range, uint32_t *__restrict__ entries,
              int *__restrict__ tile_src)
 {
-    constexpr int U = 8;
     __shared__ int scratch[33];
+    __shared__ int s_off[kWindowRows];
     __shared__ int s_cols[kChunkCols];
-    const int2 cw = chunk_win[blockIdx.x];
+    const int chunk = blockIdx.x / kTileBlocksPerChunk;
+    const int lane = threadIdx.x & 31, lr = (blockIdx.x % kTileBlocksPerChunk) * 32 + (threadIdx.x >> 5);
+    const int2 cw = chunk_win[chunk];
     const int4 wi = win_info[cw.x];
-    const int *wc = win_cols + (size_t)wi.y * kChunkCols;
     if (threadIdx.x < kChunkCols)
-        s_cols[threadIdx.x] = wc[cw.y * kChunkCols + threadIdx.x];
-    const int2 rr = row_range[(size_t)blockIdx.x * kWindowRows + threadIdx.x]; // from k_tile_count
-    const int lo = rr.x, hi = rr.y;
+        s_cols[threadIdx.x] = win_cols[((size_t)wi.y + cw.y) * kChunkCols + threadIdx.x];
+    const int len = threadIdx.x < kWindowRows ? row_range[(size_t)chunk * kWindowRows + threadIdx.x].y -
+                                                    row_range[(size_t)chunk * kWindowRows + threadIdx.x].x
+                                              : 0;
     int total;
-    const int off = block_exclusive_scan(hi - lo, &total, scratch); // its barriers also publish s_cols
-    const long long base = (long long)tile_ptr[blockIdx.x] + off;
-    const int first = s_cols[0];
-    const uint32_t lr = threadIdx.x;
-    for (int j0 = lo; j0 < hi; j0 += U) {
-        int col[U];
-        unsigned short val[U];
+    const int off = block_exclusive_scan(len, &total, scratch); // its barriers also publish s_cols
+    if (threadIdx.x < kWindowRows)
+        s_off[threadIdx.x] = off;
+    __syncthreads();
+    const int2 r = row_range[(size_t)chunk * kWindowRows + lr];
+    const long long base = (long long)tile_ptr[chunk] + s_off[lr];
+    const int n = r.y - r.x, first = s_cols[0];
+    int col[2];
+    unsigned short val[2];
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-            col[u] = j0 + u < hi ? p_col[j0 + u] : 0;
-            val[u] = j0 + u < hi ? __half_as_ushort(p_val[j0 + u]) : (unsigned short)0;
-        }
+    for (int u = 0; u < 2; u++) { // both loads before any use
+        const int k = lane + 32 * u;
+        col[u] = k < n ? p_col[r.x + k] : 0;
+        val[u] = k < n ? __half_as_ushort(p_val[r.x + k]) : (unsigned short)0;
+    }
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-            if (j0 + u >= hi)
-                break;
-            int rk;
-            if (wi.w) {
-                rk = col[u] - first; // direct chunk: 64 consecutive columns
-            } else {                 // condensed chunk: position among its ascending columns (-1 padding last)
-                int a = 0, b = kChunkCols;
-                while (a < b) {
-                    const int mid = (a + b) >> 1;
-                    const int v = s_cols[mid];
-                    if (v >= 0 && v < col[u]) a = mid + 1; else b = mid;
-                }
-                rk = a;
+    for (int u = 0; u < 2; u++) {
+        const int k = lane + 32 * u;
+        if (k >= n)
+            break;
+        int rk;
+        if (wi.w) {
+            rk = col[u] - first; // direct chunk: 64 consecutive columns
+        } else {                 // condensed chunk: position among its ascending columns (-1 padding last)
+            int a = 0, b = kChunkCols;
+            while (a < b) {
+                const int mid = (a + b) >> 1;
+                const int v = s_cols[mid];
+                if (v >= 0 && v < col[u]) a = mid + 1; else b = mid;
             }
-            entries[base + (j0 + u - lo)] = (lr << 22) | ((uint32_t)rk << 16) | (uint32_t)val[u];
-            tile_src[base + (j0 + u - lo)] = j0 + u;
+            rk = a;
         }
+        entries[base + k] = ((uint32_t)lr << 22) | ((uint32_t)rk << 16) | (uint32_t)val[u];
+        tile_src[base + k] = r.x + k;
     }
 }
 
@@ -408,6 +623,26 @@ k_render_images(const int *__restrict__ img_chunk, const int *__restrict__ tile_
 
 unsigned blocks_for(long long n, int per) { return (unsigned)((n + per - 1) / per); }
 
+int zero_async(void *p, size_t bytes, cudaStream_t s) // bytes: a multiple of 4
+{
+    const size_t n = bytes / 4;
+    if (n == 0)
+        return TCA_OK;
+    k_zero_words<<<std::min<unsigned>(blocks_for((long long)n, 256), 4 * kSMs), 256, 0, s>>>(
+        static_cast<uint32_t *>(p), n);
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
+int copy_async(const int *src, int *dst, size_t n, cudaStream_t s)
+{
+    if (n == 0)
+        return TCA_OK;
+    k_copy_words<<<std::min<unsigned>(blocks_for((long long)n, 256), 4 * kSMs), 256, 0, s>>>(src, dst, n);
+    TCA_CUDA_TRY(cudaGetLastError());
+    return TCA_OK;
+}
+
 // The stream a plan is being built on: temporaries and plan arrays are
 // stream-ordered allocations on it.
 thread_local cudaStream_t tl_build_stream = nullptr;
@@ -433,17 +668,33 @@ int dev_alloc(T **ptr, size_t count, size_t *bytes)
     return TCA_OK;
 }
 
+// Offsets of arrays sharing one allocation, each at a 256-byte boundary (a
+// pool allocation and its release cost ~2 us of host time each; a build
+// makes a handful instead of dozens).
+struct Carve {
+    size_t size = 0;
+    template <typename T>
+    size_t take(size_t count)
+    {
+        const size_t off = size;
+        size += (sizeof(T) * (count > 0 ? count : 1) + 255) & ~(size_t)255;
+        return off;
+    }
+};
+
+template <typename T>
+T *at(void *base, size_t off)
+{
+    return reinterpret_cast<T *>(static_cast<char *>(base) + off);
+}
+
 void free_plan(tca_plan *p)
 {
     if (!p) return;
     cudaDeviceSynchronize(); // the plan's arrays may still be read by queued work on any stream
     transpose_free(p);
     plan_free_fp8(p);
-    void *arrs[] = {p->perm, p->p_row_ptr, p->p_col, p->p_val, p->src, p->tc_windows, p->cc_windows,
-                    p->all_windows, p->tile_first, p->win_cols, p->tile_ptr, p->tile_entries, p->tile_src,
-                    p->img_idx, p->images, p->img_chunk, p->cc_items, p->all_items, p->tc_win_info,
-                    p->tc_pairs, p->d_status};
-    for (void *a : arrs)
+    for (void *a : p->arena)
         if (a) dev_free(a, nullptr);
     delete p;
 }
@@ -479,106 +730,145 @@ void build_items(const std::vector<int> &windows, const std::vector<int> &row_pt
 // vals_ready: an event after which `val` may be read (the host-buffer path
 // copies the values on a second stream); sync_end: wait for the whole build
 // before returning (so that the plan is usable on any stream).
+//
+// The plan's arrays come in three allocations (tca_plan::arena) and the
+// temporaries of each step in one; host-made arrays go to the device in one
+// copy per allocation. The host builds the CUDA-core work items while the
+// device writes the tiles (step 5). With vals_ready the values are gathered
+// only where they are first read (the tile entries), so that steps 1-5 run
+// while they are still on their way.
 int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *val, cudaStream_t s,
                cudaEvent_t vals_ready = nullptr, bool sync_end = true)
 {
     BuildStream build_stream(s);
     const int M = p->M, K = p->K, nnz = p->nnz;
     size_t *bytes = &p->bytes;
-    DevBuf t_row_nnz, t_row_sorted, t_err, t_iota, t_keys_out, t_p_sorted, t_scan_in, t_cub;
-    int *row_nnz, *row_sorted, *err, *iota, *keys_out, *p_sorted, *scan_in;
-    TCA_TRY(dev_alloc(&row_nnz, M, nullptr)); t_row_nnz.p = row_nnz;
-    TCA_TRY(dev_alloc(&row_sorted, M, nullptr)); t_row_sorted.p = row_sorted;
-    TCA_TRY(dev_alloc(&err, 1, nullptr)); t_err.p = err;
-    TCA_TRY(dev_alloc(&iota, M, nullptr)); t_iota.p = iota;
-    TCA_TRY(dev_alloc(&keys_out, M, nullptr)); t_keys_out.p = keys_out;
-    TCA_TRY(dev_alloc(&p_sorted, M, nullptr)); t_p_sorted.p = p_sorted;
-    TCA_TRY(dev_alloc(&scan_in, M + 1, nullptr)); t_scan_in.p = scan_in;
-
-    TCA_TRY(dev_alloc(&p->perm, M, bytes));
-    TCA_TRY(dev_alloc(&p->p_row_ptr, M + 1, bytes));
-    TCA_TRY(dev_alloc(&p->p_col, nnz, bytes));
-    TCA_TRY(dev_alloc(&p->p_val, nnz, bytes));
-    TCA_TRY(dev_alloc(&p->src, nnz, bytes));
-    TCA_TRY(dev_alloc(&p->d_status, 1, bytes));
-    TCA_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, sizeof(int), s));
-    TCA_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
-
-    // 1. checks; the host reads their verdict with the window statistics
-    // (step 3), the kernels that follow stand down on an error
-    k_row_check<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(row_ptr, col, M, K, nnz, row_nnz, row_sorted, err);
-    TCA_CUDA_TRY(cudaGetLastError());
-
-    // 2. row order
-    k_iota<<<blocks_for(M, 256), 256, 0, s>>>(iota, M);
-    if (p->opts.sort_rows) {
-        // row lengths are at most nnz: only their low bits take part
-        int end_bit = 1;
-        while (end_bit < 32 && ((long long)1 << end_bit) <= (long long)nnz) end_bit++;
-        size_t tmp = 0;
-        TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, row_nnz, keys_out, iota, p->perm, M, 0,
-                                                               end_bit, s));
-        void *tbuf;
-        TCA_TRY(dev_alloc((char **)&tbuf, tmp, nullptr)); t_cub.p = tbuf;
-        TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(tbuf, tmp, row_nnz, keys_out, iota, p->perm, M, 0,
-                                                               end_bit, s));
-    } else {
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->perm, iota, sizeof(int) * M, cudaMemcpyDeviceToDevice, s));
-    }
-    TCA_CUDA_TRY(cudaMemsetAsync(scan_in + M, 0, sizeof(int), s));
-    k_gather_int<<<blocks_for(M, 256), 256, 0, s>>>(row_nnz, p->perm, scan_in, M);
-    k_gather_int<<<blocks_for(M, 256), 256, 0, s>>>(row_sorted, p->perm, p_sorted, M);
-    {
-        size_t tmp = 0;
-        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, scan_in, p->p_row_ptr, M + 1, s));
-        DevBuf tb;
-        char *tbuf;
-        TCA_TRY(dev_alloc(&tbuf, tmp, nullptr)); tb.p = tbuf;
-        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tbuf, tmp, scan_in, p->p_row_ptr, M + 1, s));
-    } // tb is released in stream order on s (DevBuf): no wait
-    if (vals_ready)
-        TCA_CUDA_TRY(cudaStreamWaitEvent(s, vals_ready, 0));
-    k_permute<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(p->perm, row_ptr, col, val, p->p_row_ptr, M, err,
-                                                                 p->p_col, p->p_val, p->src);
-    TCA_CUDA_TRY(cudaGetLastError());
-
-    // 3. windows. The host reads, in one copy after one wait, everything it
-    // decides on: per window its distinct columns, nonzeros, sortedness and
-    // touched 64-column blocks, the check verdict and the sorted row offsets
-    // (for the work items, step 7), gathered in one device array.
     const int W = (M + kWindowRows - 1) / kWindowRows;
     p->n_windows = W;
-    std::vector<int> h_all(W);
-    for (int w = 0; w < W; w++) h_all[w] = w;
-    TCA_TRY(dev_alloc(&p->all_windows, W, bytes));
-    TCA_CUDA_TRY(cudaMemcpyAsync(p->all_windows, h_all.data(), sizeof(int) * W, cudaMemcpyHostToDevice, s));
-
-    const size_t n_stage = 4 * (size_t)W + 1 + (size_t)M + 1;
-    DevBuf t_stage;
-    int *d_stage;
-    TCA_TRY(dev_alloc(&d_stage, n_stage, nullptr)); t_stage.p = d_stage;
-    int *d_nu = d_stage, *d_wn = d_stage + W, *d_el = d_stage + 2 * W, *d_nb = d_stage + 3 * W;
+    const bool small = M <= kOrderRows;
     const bool tc_possible = (p->opts.path != 1) && K <= kMaxTcK && K > 0 && W > 0;
     // the windows' column bitmaps, kept from the statistics for the tile
     // columns when they take at most 64 MB (else k_tile_cols rebuilds them)
-    DevBuf t_bm;
-    uint32_t *d_bm = nullptr;
-    if (tc_possible && (size_t)W * ((K + 31) / 32) <= (size_t)(16u << 20)) {
-        TCA_TRY(dev_alloc(&d_bm, (size_t)W * ((K + 31) / 32), nullptr));
-        t_bm.p = d_bm;
+    const size_t bm_words = (size_t)W * ((K + 31) / 32);
+    const bool keep_bm = tc_possible && bm_words <= (size_t)(16u << 20);
+
+    {
+        Carve c;
+        const size_t o_perm = c.take<int>(M), o_rp = c.take<int>((size_t)M + 1), o_col = c.take<int>(nnz),
+                     o_val = c.take<__half>(nnz), o_src = c.take<int>(nnz), o_status = c.take<int>(1),
+                     o_all = c.take<int>(W);
+        char *a;
+        TCA_TRY(dev_alloc(&a, c.size, bytes));
+        p->arena[0] = a;
+        p->perm = at<int>(a, o_perm);
+        p->p_row_ptr = at<int>(a, o_rp);
+        p->p_col = at<int>(a, o_col);
+        p->p_val = at<__half>(a, o_val);
+        p->src = at<int>(a, o_src);
+        p->d_status = at<int>(a, o_status);
+        p->all_windows = at<int>(a, o_all);
     }
-    if (tc_possible) {
+
+    // temporaries of steps 1-3; the stage array gathers what the host reads
+    // after step 3: per window its distinct columns, nonzeros, sortedness and
+    // touched 64-column blocks, then the check verdict and the sorted row
+    // offsets (for the work items)
+    const size_t n_stage = 4 * (size_t)W + 1 + (size_t)M + 1;
+    int end_bit = 1; // row lengths are at most nnz: only their low bits take part
+    while (end_bit < 32 && ((long long)1 << end_bit) <= (long long)nnz) end_bit++;
+    size_t sort_tmp = 0, scan_tmp = 0;
+    if (!small) {
+        if (p->opts.sort_rows)
+            TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_tmp, (const int *)nullptr,
+                                                                   (int *)nullptr, (const int *)nullptr,
+                                                                   (int *)nullptr, M, 0, end_bit, s));
+        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (const int *)nullptr, (int *)nullptr, M + 1, s));
+    }
+    // err, the per-window block counters of step 3 and the kept bitmaps are
+    // adjacent: one memset clears them
+    Carve ct;
+    const size_t o_nnz = ct.take<int>(M), o_sorted = ct.take<int>(M), o_psorted = ct.take<int>(M),
+                 o_stage = ct.take<int>(n_stage), o_err = ct.take<int>(1 + (size_t)W),
+                 o_bm = ct.take<uint32_t>(keep_bm ? bm_words : 0);
+    const size_t zero_bytes = keep_bm ? o_bm - o_err + sizeof(uint32_t) * bm_words : sizeof(int) * (1 + (size_t)W);
+    size_t o_iota = 0, o_keys = 0, o_scan_in = 0, o_sort_tmp = 0, o_scan_tmp = 0;
+    if (!small) {
+        o_iota = ct.take<int>(M);
+        o_keys = ct.take<int>(M);
+        o_scan_in = ct.take<int>((size_t)M + 1);
+        o_sort_tmp = ct.take<char>(sort_tmp);
+        o_scan_tmp = ct.take<char>(scan_tmp);
+    }
+    DevBuf t_steps13;
+    char *tb;
+    TCA_TRY(dev_alloc(&tb, ct.size, nullptr));
+    t_steps13.p = tb;
+    int *row_nnz = at<int>(tb, o_nnz), *row_sorted = at<int>(tb, o_sorted), *err = at<int>(tb, o_err);
+    int *p_sorted = at<int>(tb, o_psorted), *d_stage = at<int>(tb, o_stage);
+    uint32_t *d_bm = keep_bm ? at<uint32_t>(tb, o_bm) : nullptr;
+    int *d_done = err + 1;
+    TCA_TRY(zero_async(err, zero_bytes, s));
+
+    // 1. checks; the host reads their verdict with the window statistics
+    // (step 3), the kernels that follow stand down on an error
+    k_row_check<<<blocks_for(std::max((long long)M * 32, (long long)W), 256), 256, 0, s>>>(
+        row_ptr, col, M, K, nnz, row_nnz, row_sorted, err, p->all_windows, W, p->d_status);
+    TCA_CUDA_TRY(cudaGetLastError());
+
+    // 2. row order
+    if (small) {
+        k_order_small<<<1, kOrderThreads, 0, s>>>(row_nnz, row_sorted, M, p->opts.sort_rows ? 1 : 0, err, p->perm,
+                                                  p->p_row_ptr, p_sorted, d_stage + 4 * W, d_stage + 4 * W + 1);
+    } else {
+        int *iota = at<int>(tb, o_iota), *keys_out = at<int>(tb, o_keys), *scan_in = at<int>(tb, o_scan_in);
+        k_iota<<<blocks_for(M, 256), 256, 0, s>>>(iota, M);
+        if (p->opts.sort_rows)
+            TCA_CUDA_TRY(cub::DeviceRadixSort::SortPairsDescending(at<char>(tb, o_sort_tmp), sort_tmp, row_nnz,
+                                                                   keys_out, iota, p->perm, M, 0, end_bit, s));
+        else
+            TCA_TRY(copy_async(iota, p->perm, M, s));
+        TCA_TRY(zero_async(scan_in + M, sizeof(int), s));
+        k_gather_int<<<blocks_for(M, 256), 256, 0, s>>>(row_nnz, p->perm, scan_in, M);
+        k_gather_int<<<blocks_for(M, 256), 256, 0, s>>>(row_sorted, p->perm, p_sorted, M);
+        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at<char>(tb, o_scan_tmp), scan_tmp, scan_in, p->p_row_ptr, M + 1, s));
+        TCA_TRY(copy_async(err, d_stage + 4 * W, 1, s));
+        TCA_TRY(copy_async(p->p_row_ptr, d_stage + 4 * W + 1, (size_t)M + 1, s));
+    }
+    TCA_CUDA_TRY(cudaGetLastError());
+    bool vals_later = vals_ready != nullptr;
+    k_permute<<<blocks_for((long long)M * 32, 256), 256, 0, s>>>(p->perm, row_ptr, col, vals_later ? nullptr : val,
+                                                                 p->p_row_ptr, M, err, p->p_col, p->p_val, p->src);
+    TCA_CUDA_TRY(cudaGetLastError());
+    // after the host has seen a clean check (src is then complete)
+    auto gather_vals = [&]() -> int {
+        if (!vals_later)
+            return TCA_OK;
+        vals_later = false;
+        TCA_CUDA_TRY(cudaStreamWaitEvent(s, vals_ready, 0));
+        if (nnz > 0)
+            k_update_p_val<<<blocks_for(nnz, 256), 256, 0, s>>>(p->src, val, p->p_val, nnz);
+        TCA_CUDA_TRY(cudaGetLastError());
+        return TCA_OK;
+    };
+
+    // 3. windows
+    int *d_nu = d_stage, *d_wn = d_stage + W, *d_el = d_stage + 2 * W, *d_nb = d_stage + 3 * W;
+    if (tc_possible && keep_bm) {
+        // about two blocks per SM, each with at least ~4K nonzeros
+        const long long per_window = (long long)nnz / W;
+        const int split = std::max(1, std::min((2 * kSMs + W - 1) / W, (int)std::min(64LL, per_window / 4096)));
+        const size_t smem = sizeof(uint32_t) * ((K + 31) / 32); // at most 16 KB (K <= kMaxTcK)
+        k_window_stats_split<<<W * split, 512, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, err, split, d_nu,
+                                                          d_wn, d_el, d_nb, d_bm, d_done);
+        TCA_CUDA_TRY(cudaGetLastError());
+    } else if (tc_possible) {
         const size_t smem = sizeof(uint32_t) * ((K + 31) / 32);
-        TCA_CUDA_TRY(cudaFuncSetAttribute(k_window_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_window_stats<<<W, 1024, smem, s>>>(p->p_row_ptr, p->p_col, p_sorted, M, K, err, d_nu, d_wn, d_el, d_nb,
-                                             d_bm);
+                                             nullptr);
         TCA_CUDA_TRY(cudaGetLastError());
     } else if (W > 0) {
-        TCA_CUDA_TRY(cudaMemsetAsync(d_stage, 0, sizeof(int) * 4 * (size_t)W, s));
+        TCA_TRY(zero_async(d_stage, sizeof(int) * 4 * (size_t)W, s));
     }
-    TCA_CUDA_TRY(cudaMemcpyAsync(d_stage + 4 * W, err, sizeof(int), cudaMemcpyDeviceToDevice, s));
-    TCA_CUDA_TRY(cudaMemcpyAsync(d_stage + 4 * W + 1, p->p_row_ptr, sizeof(int) * ((size_t)M + 1),
-                                 cudaMemcpyDeviceToDevice, s));
     std::vector<int> h_stage(n_stage);
     TCA_CUDA_TRY(cudaMemcpyAsync(h_stage.data(), d_stage, sizeof(int) * n_stage, cudaMemcpyDeviceToHost, s));
     TCA_CUDA_TRY(cudaStreamSynchronize(s));
@@ -624,26 +914,16 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
     p->n_tc_chunks = h_first.back();
     p->h_tile_first = h_first;
     p->tc_nnz = ebase;
-    TCA_TRY(dev_alloc(&p->tc_windows, p->n_tc, bytes));
-    TCA_TRY(dev_alloc(&p->cc_windows, p->n_cc, bytes));
-    TCA_TRY(dev_alloc(&p->tile_first, p->n_tc + 1, bytes));
-    if (p->n_tc)
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->tc_windows, tc_list.data(), sizeof(int) * p->n_tc, cudaMemcpyHostToDevice, s));
-    if (p->n_cc)
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->cc_windows, cc_list.data(), sizeof(int) * p->n_cc, cudaMemcpyHostToDevice, s));
-    TCA_CUDA_TRY(cudaMemcpyAsync(p->tile_first, h_first.data(), sizeof(int) * (p->n_tc + 1), cudaMemcpyHostToDevice, s));
-    std::vector<int4> h_wi((size_t)p->n_tc);
-    for (int t = 0; t < p->n_tc; t++)
+    const int n_tc = p->n_tc, n_ch = p->n_tc_chunks;
+    std::vector<int4> h_wi((size_t)n_tc);
+    for (int t = 0; t < n_tc; t++)
         h_wi[t] = make_int4(tc_list[t], h_first[t], h_first[t + 1] - h_first[t], h_direct[t]);
-    TCA_TRY(dev_alloc(&p->tc_win_info, (size_t)p->n_tc, bytes));
-    if (p->n_tc)
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->tc_win_info, h_wi.data(), sizeof(int4) * p->n_tc, cudaMemcpyHostToDevice, s));
     // window pairs for the pair kernel: greedily, consecutive windows whose
     // chunks are all 64-column blocks of K (identical columns)
     std::vector<int2> h_pairs;
     p->n_full_pairs = 0;
-    for (int t = 0; t < p->n_tc;) {
-        if (h_full[t] && t + 1 < p->n_tc && h_full[t + 1]) {
+    for (int t = 0; t < n_tc;) {
+        if (h_full[t] && t + 1 < n_tc && h_full[t + 1]) {
             h_pairs.push_back(make_int2(t, t + 1));
             p->n_full_pairs++;
             t += 2;
@@ -653,86 +933,131 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         }
     }
     p->n_pairs = (int)h_pairs.size();
-    TCA_TRY(dev_alloc(&p->tc_pairs, (size_t)p->n_pairs, bytes));
-    if (p->n_pairs)
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->tc_pairs, h_pairs.data(), sizeof(int2) * p->n_pairs, cudaMemcpyHostToDevice, s));
+    // chunk -> (tensor-core window, chunk within the window)
+    std::vector<int2> h_cw;
+    h_cw.reserve((size_t)n_ch);
+    for (int t = 0; t < n_tc; t++)
+        for (int c = 0; c < h_wi[t].z; c++) h_cw.push_back(make_int2(t, c));
+
+    // the window lists (made here, copied in one piece) and the tiles
+    int2 *d_cw;
+    {
+        Carve c;
+        const size_t o_tcw = c.take<int>(n_tc), o_ccw = c.take<int>(p->n_cc), o_first = c.take<int>(n_tc + 1),
+                     o_wi = c.take<int4>(n_tc), o_pairs = c.take<int2>(p->n_pairs), o_cw = c.take<int2>(n_ch);
+        const size_t host_part = c.size;
+        const size_t o_wc = c.take<int>((size_t)n_ch * kChunkCols), o_tp = c.take<int>((size_t)n_ch + 1),
+                     o_te = c.take<uint32_t>((size_t)p->tc_nnz + kEntryPad), o_ts = c.take<int>((size_t)p->tc_nnz);
+        char *a;
+        TCA_TRY(dev_alloc(&a, c.size, bytes));
+        p->arena[1] = a;
+        p->tc_windows = at<int>(a, o_tcw);
+        p->cc_windows = at<int>(a, o_ccw);
+        p->tile_first = at<int>(a, o_first);
+        p->tc_win_info = at<int4>(a, o_wi);
+        p->tc_pairs = at<int2>(a, o_pairs);
+        d_cw = at<int2>(a, o_cw);
+        p->win_cols = at<int>(a, o_wc);
+        p->tile_ptr = at<int>(a, o_tp);
+        p->tile_entries = at<uint32_t>(a, o_te);
+        p->tile_src = at<int>(a, o_ts);
+        std::vector<char> h_part(host_part);
+        auto put = [&](size_t off, const void *src, size_t n) { if (n) std::memcpy(h_part.data() + off, src, n); };
+        put(o_tcw, tc_list.data(), sizeof(int) * n_tc);
+        put(o_ccw, cc_list.data(), sizeof(int) * p->n_cc);
+        put(o_first, h_first.data(), sizeof(int) * (n_tc + 1));
+        put(o_wi, h_wi.data(), sizeof(int4) * n_tc);
+        put(o_pairs, h_pairs.data(), sizeof(int2) * p->n_pairs);
+        put(o_cw, h_cw.data(), sizeof(int2) * n_ch);
+        // pageable: the copy returns once its source is staged
+        TCA_CUDA_TRY(cudaMemcpyAsync(a, h_part.data(), host_part, cudaMemcpyHostToDevice, s));
+    }
+    TCA_TRY(zero_async(p->tile_entries + p->tc_nnz, sizeof(uint32_t) * kEntryPad, s));
 
     // 5. tiles
-    TCA_TRY(dev_alloc(&p->win_cols, (size_t)p->n_tc_chunks * kChunkCols, bytes));
-    TCA_TRY(dev_alloc(&p->tile_ptr, (size_t)p->n_tc_chunks + 1, bytes));
-    TCA_TRY(dev_alloc(&p->tile_entries, (size_t)p->tc_nnz + kEntryPad, bytes));
-    TCA_CUDA_TRY(cudaMemsetAsync(p->tile_entries + p->tc_nnz, 0, sizeof(uint32_t) * kEntryPad, s));
-    TCA_TRY(dev_alloc(&p->tile_src, (size_t)p->tc_nnz, bytes));
-    if (p->n_tc > 0) {
-        // chunk -> (tensor-core window, chunk within the window)
-        std::vector<int2> h_cw;
-        h_cw.reserve((size_t)p->n_tc_chunks);
-        for (int t = 0; t < p->n_tc; t++)
-            for (int c = 0; c < h_wi[t].z; c++) h_cw.push_back(make_int2(t, c));
-        DevBuf t_cw, t_cn, t_scan, t_rr;
-        int2 *d_cw, *d_rr;
-        int *d_cn;
-        TCA_TRY(dev_alloc(&d_cw, (size_t)p->n_tc_chunks, nullptr)); t_cw.p = d_cw;
-        TCA_TRY(dev_alloc(&d_cn, (size_t)p->n_tc_chunks + 1, nullptr)); t_cn.p = d_cn;
-        TCA_TRY(dev_alloc(&d_rr, (size_t)p->n_tc_chunks * kWindowRows, nullptr)); t_rr.p = d_rr;
-        TCA_CUDA_TRY(cudaMemcpyAsync(d_cw, h_cw.data(), sizeof(int2) * h_cw.size(), cudaMemcpyHostToDevice, s));
-        TCA_CUDA_TRY(cudaMemsetAsync(d_cn + p->n_tc_chunks, 0, sizeof(int), s));
+    DevBuf t_step5;
+    std::vector<int> h_ptr((size_t)n_ch + 1, 0);
+    if (n_tc > 0) {
+        const bool small_scan = n_ch <= kScanSmallMax;
+        size_t tmp = 0;
+        if (!small_scan)
+            TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, (const int *)nullptr, (int *)nullptr, n_ch + 1, s));
+        Carve c;
+        const size_t o_cn = c.take<int>((size_t)n_ch + 1), o_rr = c.take<int2>((size_t)n_ch * kWindowRows),
+                     o_tmp = c.take<char>(tmp);
+        char *tb5;
+        TCA_TRY(dev_alloc(&tb5, c.size, nullptr));
+        t_step5.p = tb5;
+        int *d_cn = at<int>(tb5, o_cn);
+        int2 *d_rr = at<int2>(tb5, o_rr);
         const size_t smem = 2 * sizeof(uint32_t) * ((K + 31) / 32);
         TCA_CUDA_TRY(cudaFuncSetAttribute(k_tile_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_tile_cols<<<p->n_tc, 1024, smem, s>>>(p->tc_win_info, p->p_row_ptr, p->p_col, M, K, d_bm, p->win_cols);
-        k_tile_count<<<p->n_tc_chunks, 128, 0, s>>>(d_cw, p->tc_win_info, p->p_row_ptr, p->p_col, p->win_cols, M,
-                                                    d_cn, d_rr);
-        size_t tmp = 0;
-        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_cn, p->tile_ptr, p->n_tc_chunks + 1, s));
-        void *tb;
-        TCA_TRY(dev_alloc((char **)&tb, tmp, nullptr)); t_scan.p = tb;
-        TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tb, tmp, d_cn, p->tile_ptr, p->n_tc_chunks + 1, s));
-        k_tile_write<<<p->n_tc_chunks, 128, 0, s>>>(d_cw, p->tc_win_info, p->p_col, p->p_val, p->win_cols,
-                                                    p->tile_ptr, d_rr, p->tile_entries, p->tile_src);
+        k_tile_cols<<<n_tc, 1024, smem, s>>>(p->tc_win_info, p->p_row_ptr, p->p_col, M, K, d_bm, p->win_cols);
+        TCA_TRY(zero_async(d_cn, sizeof(int) * ((size_t)n_ch + 1), s));
+        k_tile_count<<<(unsigned)n_ch * kTileBlocksPerChunk, 1024, 0, s>>>(d_cw, p->tc_win_info, p->p_row_ptr,
+                                                                           p->p_col, p->win_cols, M, d_cn, d_rr);
+        if (small_scan) {
+            k_scan_small<<<1, kScanThreads, 0, s>>>(d_cn, n_ch, p->tile_ptr);
+        } else {
+            TCA_CUDA_TRY(cub::DeviceScan::ExclusiveSum(at<char>(tb5, o_tmp), tmp, d_cn, p->tile_ptr, n_ch + 1, s));
+        }
+        TCA_TRY(gather_vals());
+        k_tile_write<<<(unsigned)n_ch * kTileBlocksPerChunk, 1024, 0, s>>>(d_cw, p->tc_win_info, p->p_col, p->p_val,
+                                                                           p->win_cols, p->tile_ptr, d_rr,
+                                                                           p->tile_entries, p->tile_src);
         TCA_CUDA_TRY(cudaGetLastError());
     } else {
-        TCA_CUDA_TRY(cudaMemsetAsync(p->tile_ptr, 0, sizeof(int), s));
+        TCA_TRY(zero_async(p->tile_ptr, sizeof(int), s));
     }
 
+    // 7 (while the device writes the tiles). CUDA-core work items.
+    std::vector<int> h_all(W);
+    for (int w = 0; w < W; w++) h_all[w] = w;
+    std::vector<int2> cc_items, all_items;
+    build_items(cc_list, h_rp, M, cc_items);
+    build_items(h_all, h_rp, M, all_items);
+    p->n_cc_items = (int)cc_items.size();
+    p->n_all_items = (int)all_items.size();
+
     // 6. dense tile images for chunks holding at least kImageMinNnz nonzeros
-    std::vector<int> h_ptr((size_t)p->n_tc_chunks + 1, 0), h_img((size_t)p->n_tc_chunks, -1), h_img_chunk;
-    if (p->n_tc_chunks > 0)
+    if (n_ch > 0) {
         TCA_CUDA_TRY(cudaMemcpyAsync(h_ptr.data(), p->tile_ptr, sizeof(int) * h_ptr.size(), cudaMemcpyDeviceToHost, s));
-    TCA_CUDA_TRY(cudaStreamSynchronize(s));
-    for (int c = 0; c < p->n_tc_chunks; c++)
+        TCA_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    std::vector<int> h_img((size_t)n_ch, -1), h_img_chunk;
+    for (int c = 0; c < n_ch; c++)
         if (h_ptr[c + 1] - h_ptr[c] >= kImageMinNnz) {
             h_img[c] = (int)h_img_chunk.size();
             h_img_chunk.push_back(c);
         }
     p->n_images = (int)h_img_chunk.size();
-    TCA_TRY(dev_alloc(&p->img_idx, (size_t)p->n_tc_chunks, bytes));
-    TCA_TRY(dev_alloc(&p->img_chunk, (size_t)p->n_images, bytes));
-    TCA_TRY(dev_alloc(&p->images, (size_t)p->n_images * kWindowRows * kChunkCols, bytes));
-    if (p->n_tc_chunks > 0)
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->img_idx, h_img.data(), sizeof(int) * h_img.size(), cudaMemcpyHostToDevice, s));
+    {
+        Carve c;
+        const size_t o_idx = c.take<int>(n_ch), o_ich = c.take<int>(p->n_images),
+                     o_cci = c.take<int2>(cc_items.size()), o_alli = c.take<int2>(all_items.size());
+        const size_t host_part = c.size;
+        const size_t o_img = c.take<uint16_t>((size_t)p->n_images * kWindowRows * kChunkCols);
+        char *a;
+        TCA_TRY(dev_alloc(&a, c.size, bytes));
+        p->arena[2] = a;
+        p->img_idx = at<int>(a, o_idx);
+        p->img_chunk = at<int>(a, o_ich);
+        p->cc_items = at<int2>(a, o_cci);
+        p->all_items = at<int2>(a, o_alli);
+        p->images = at<uint16_t>(a, o_img);
+        std::vector<char> h_part(host_part);
+        auto put = [&](size_t off, const void *src, size_t n) { if (n) std::memcpy(h_part.data() + off, src, n); };
+        put(o_idx, h_img.data(), sizeof(int) * h_img.size());
+        put(o_ich, h_img_chunk.data(), sizeof(int) * h_img_chunk.size());
+        put(o_cci, cc_items.data(), sizeof(int2) * cc_items.size());
+        put(o_alli, all_items.data(), sizeof(int2) * all_items.size());
+        TCA_CUDA_TRY(cudaMemcpyAsync(a, h_part.data(), host_part, cudaMemcpyHostToDevice, s));
+    }
     if (p->n_images > 0) {
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->img_chunk, h_img_chunk.data(), sizeof(int) * h_img_chunk.size(),
-                                     cudaMemcpyHostToDevice, s));
         k_render_images<<<p->n_images, 256, 0, s>>>(p->img_chunk, p->tile_ptr, p->tile_entries, p->images);
         TCA_CUDA_TRY(cudaGetLastError());
     }
-
-    // 7. CUDA-core work items. The host arrays copied to the device here (and
-    // above) are pageable, so a copy returns once its data is staged; each
-    // copy still has a source array of its own.
-    std::vector<int2> cc_items, all_items;
-    build_items(cc_list, h_rp, M, cc_items);
-    p->n_cc_items = (int)cc_items.size();
-    TCA_TRY(dev_alloc(&p->cc_items, cc_items.size(), bytes));
-    if (!cc_items.empty())
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->cc_items, cc_items.data(), sizeof(int2) * cc_items.size(),
-                                     cudaMemcpyHostToDevice, s));
-    build_items(h_all, h_rp, M, all_items);
-    p->n_all_items = (int)all_items.size();
-    TCA_TRY(dev_alloc(&p->all_items, all_items.size(), bytes));
-    if (!all_items.empty())
-        TCA_CUDA_TRY(cudaMemcpyAsync(p->all_items, all_items.data(), sizeof(int2) * all_items.size(),
-                                     cudaMemcpyHostToDevice, s));
+    TCA_TRY(gather_vals());
     if (sync_end)
         TCA_CUDA_TRY(cudaStreamSynchronize(s)); // the plan is complete, for work on any stream
     return TCA_OK;

@@ -68,6 +68,12 @@ struct tca_plan {
     // (n_tc + 1), for sizing launches on the host
     std::vector<int> h_tile_first;
     int *d_status = nullptr; // device error word written by bounded waits
+    // The arrays above live in three device allocations, made when their
+    // sizes become known: [0] the re-ordered CSR (perm .. src, d_status,
+    // all_windows), [1] the window lists and tiles (tc_windows .. tile_src),
+    // [2] the images and work items (img_idx, img_chunk, cc_items,
+    // all_items, images).
+    void *arena[3] = {nullptr, nullptr, nullptr};
     size_t bytes = 0;
     // A^T as a plan of its own (built on first use by tca_spmm_t or by
     // tca_plan_build_transpose), with t_src mapping each of its entries to the

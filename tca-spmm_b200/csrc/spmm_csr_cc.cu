@@ -255,12 +255,16 @@ struct CcJob {
     unsigned flags;
 };
 
-struct CcBatch {
+// A launch's jobs; the stream kernel is also built for CAP = 1, whose
+// parameter block launches faster for a single forward.
+template <int CAP>
+struct CcBatchT {
     int n_jobs;
-    int block_start[kMaxCcJobs + 1]; // first block of each job (spmm_cc_items_kernel)
-    int item_start[kMaxCcJobs + 1];  // first item of each job in the flattened list (spmm_cc_stream_kernel)
-    CcJob job[kMaxCcJobs];
+    int block_start[CAP + 1]; // first block of each job (spmm_cc_items_kernel)
+    int item_start[CAP + 1];  // first item of each job in the flattened list (spmm_cc_stream_kernel)
+    CcJob job[CAP];
 };
+using CcBatch = CcBatchT<kMaxCcJobs>;
 
 template <typename OutT, int L, bool VEC>
 __global__ void __launch_bounds__(256) spmm_cc_items_kernel(const __grid_constant__ CcBatch b)
@@ -424,7 +428,8 @@ struct ItemDesc {
     int job, r0, nrows; // nrows == 0: no item
 };
 
-__device__ __forceinline__ ItemDesc load_desc(const CcBatch &b, int item)
+template <typename Batch>
+__device__ __forceinline__ ItemDesc load_desc(const Batch &b, int item)
 {
     ItemDesc d{0, 0, 0};
     if (item < b.item_start[b.n_jobs]) {
@@ -506,8 +511,8 @@ __device__ __forceinline__ void fma_vec(float *acc, unsigned short v, const V &b
 // from its SM sub-partition, and the tensor-core warps leave room for two
 // more warps per sub-partition). U B loads are in flight per lane: 8, or 4
 // at W = 8, which keeps the register budget without spills.
-template <typename OutT, int W, bool F8>
-__global__ void __launch_bounds__(256, 3) spmm_cc_stream_kernel(const __grid_constant__ CcBatch b)
+template <typename OutT, int W, bool F8, int CAP = kMaxCcJobs>
+__global__ void __launch_bounds__(256, 3) spmm_cc_stream_kernel(const __grid_constant__ CcBatchT<CAP> b)
 {
     using V = typename BVec<W, F8>::T;
     constexpr int U = W == 8 ? 4 : 8;
@@ -1003,8 +1008,8 @@ __global__ void __launch_bounds__(kMmaWarps * 32, 2) spmm_cc_mma_kernel(const __
 // faster than both a wider first block and claiming items from a counter
 // with more blocks). The kernel reads nothing the tensor-core kernel writes,
 // so it never waits on it.
-template <typename OutT, int W, bool F8>
-int launch_stream_group(const CcBatch &b, int beside_regs, cudaStream_t s)
+template <typename OutT, int W, bool F8, int CAP>
+int launch_stream_cap(const CcBatchT<CAP> &b, int beside_regs, cudaStream_t s)
 {
     const int total = b.item_start[b.n_jobs];
     if (b.n_jobs == 0 || total == 0)
@@ -1012,8 +1017,8 @@ int launch_stream_group(const CcBatch &b, int beside_regs, cudaStream_t s)
     static int per_sm = 0, regs = 0;
     if (per_sm == 0) {
         int n = 0;
-        TCA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spmm_cc_stream_kernel<OutT, W, F8>, 256, 0));
-        TCA_TRY(block_regs((const void *)spmm_cc_stream_kernel<OutT, W, F8>, 256, &regs));
+        TCA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spmm_cc_stream_kernel<OutT, W, F8, CAP>, 256, 0));
+        TCA_TRY(block_regs((const void *)spmm_cc_stream_kernel<OutT, W, F8, CAP>, 256, &regs));
         per_sm = n > 0 ? n : 1;
     }
     const int fit = beside_regs > 0 ? std::max(1, std::min(per_sm, (kSmRegs - beside_regs) / regs)) : per_sm;
@@ -1028,12 +1033,28 @@ int launch_stream_group(const CcBatch &b, int beside_regs, cudaStream_t s)
         attr[0].val.programmaticStreamSerializationAllowed = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        TCA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmm_cc_stream_kernel<OutT, W, F8>, b));
+        TCA_CUDA_TRY(cudaLaunchKernelEx(&cfg, spmm_cc_stream_kernel<OutT, W, F8, CAP>, b));
         return TCA_OK;
     }
-    spmm_cc_stream_kernel<OutT, W, F8><<<grid, 256, 0, s>>>(b);
+    spmm_cc_stream_kernel<OutT, W, F8, CAP><<<grid, 256, 0, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
+}
+
+template <typename OutT, int W, bool F8>
+int launch_stream_group(const CcBatch &b, int beside_regs, cudaStream_t s)
+{
+    if (b.n_jobs == 1) {
+        CcBatchT<1> one;
+        one.n_jobs = 1;
+        one.block_start[0] = b.block_start[0];
+        one.block_start[1] = b.block_start[1];
+        one.item_start[0] = b.item_start[0];
+        one.item_start[1] = b.item_start[1];
+        one.job[0] = b.job[0];
+        return launch_stream_cap<OutT, W, F8, 1>(one, beside_regs, s);
+    }
+    return launch_stream_cap<OutT, W, F8, kMaxCcJobs>(b, beside_regs, s);
 }
 
 template <typename OutT>

@@ -77,11 +77,16 @@ struct TcJob {
     unsigned flags;
 };
 
-struct TcBatch {
+// A launch's jobs. The kernel is also built for CAP = 1: a single forward's
+// parameter block is then ~0.4 KB instead of ~12 KB (measured: the launch
+// took 5-15 us of host time with the full block).
+template <int CAP>
+struct TcBatchT {
     int n_jobs;
-    int item_start[kMaxJobs + 1];
-    TcJob job[kMaxJobs];
+    int item_start[CAP + 1];
+    TcJob job[CAP];
 };
+using TcBatch = TcBatchT<kMaxJobs>;
 
 using namespace ptx;
 
@@ -171,7 +176,8 @@ template <int NT, bool F8> struct TcCfg {
 
 // Work item (job, tensor-core window, N slice) -> table entry {window,
 // first chunk, chunk count, job << 16 | N-slice index}.
-__device__ __forceinline__ int4 decode_item(const TcBatch &batch, int item)
+template <typename Batch>
+__device__ __forceinline__ int4 decode_item(const Batch &batch, int item)
 {
     int j = 0;
     while (j + 1 < batch.n_jobs && batch.item_start[j + 1] <= item) j++;
@@ -210,8 +216,8 @@ __device__ __forceinline__ int4 decode_item(const TcBatch &batch, int item)
 //   warps 6-9 (epilogue): per item wait "accum_full", tcgen05.ld the rows
 //     (warp w reads TMEM lanes 32 (w % 4) ..), alpha/beta, store to C[perm],
 //     arrive "accum_empty" -- overlapping the next item's main loop.
-template <int NT, typename OutT, bool F8>
-__global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_constant__ TcBatch batch)
+template <int NT, typename OutT, bool F8, int CAP = kMaxJobs>
+__global__ void __launch_bounds__(kThreads, 1) spmm_tc_kernel(const __grid_constant__ TcBatchT<CAP> batch)
 {
     using Cfg = TcCfg<NT, F8>;
     constexpr int S = Cfg::kStages;
@@ -1049,23 +1055,39 @@ int make_job(const SpmmJob &sj, float alpha, float beta, unsigned flags, int NT,
     return TCA_OK;
 }
 
-template <int NT, typename OutT, bool F8>
-int launch_group(const TcBatch &b, cudaStream_t s)
+template <int NT, typename OutT, bool F8, int CAP>
+int launch_group_cap(const TcBatchT<CAP> &b, cudaStream_t s)
 {
     const int smem = TcCfg<NT, F8>::kSmem;
-    TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT, F8, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem));
     // The whole 228 KB carveout: with the smallest one that holds this block
     // (196 KB for the E4M3 rings) no room is left for the 1 KB that each
     // CUDA-core block reserves, and the launch that should run beside this
     // one waits for it to end (measured: E4M3 step, CUDA-core blocks starting
     // as the first tensor-core blocks exit).
-    TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT, F8>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    TCA_CUDA_TRY(cudaFuncSetAttribute(spmm_tc_kernel<NT, OutT, F8, CAP>,
+                                      cudaFuncAttributePreferredSharedMemoryCarveout,
                                       (int)cudaSharedmemCarveoutMaxShared));
     const int total = b.item_start[b.n_jobs];
     const int grid = std::min(total, std::max(kSMs, (total + kMaxCtaItems - 1) / kMaxCtaItems));
-    spmm_tc_kernel<NT, OutT, F8><<<grid, kThreads, smem, s>>>(b);
+    spmm_tc_kernel<NT, OutT, F8, CAP><<<grid, kThreads, smem, s>>>(b);
     TCA_CUDA_TRY(cudaGetLastError());
     return TCA_OK;
+}
+
+template <int NT, typename OutT, bool F8>
+int launch_group(const TcBatch &b, cudaStream_t s)
+{
+    if (b.n_jobs == 1) {
+        TcBatchT<1> one;
+        one.n_jobs = 1;
+        one.item_start[0] = b.item_start[0];
+        one.item_start[1] = b.item_start[1];
+        one.job[0] = b.job[0];
+        return launch_group_cap<NT, OutT, F8, 1>(one, s);
+    }
+    return launch_group_cap<NT, OutT, F8, kMaxJobs>(b, s);
 }
 
 template <typename OutT>
@@ -1159,11 +1181,16 @@ int tc_block_regs(bool f8, int *regs)
             (const void *)spmm_tc_kernel<64, __half, false>, (const void *)spmm_tc_kernel<128, __half, false>,
             (const void *)spmm_tc_kernel<256, __half, false>, (const void *)spmm_tc_kernel<64, float, false>,
             (const void *)spmm_tc_kernel<128, float, false>, (const void *)spmm_tc_kernel<256, float, false>,
-            (const void *)spmm_tc_pair_kernel<__half, false>, (const void *)spmm_tc_pair_kernel<float, false>};
+            (const void *)spmm_tc_pair_kernel<__half, false>, (const void *)spmm_tc_pair_kernel<float, false>,
+            (const void *)spmm_tc_kernel<64, __half, false, 1>, (const void *)spmm_tc_kernel<128, __half, false, 1>,
+            (const void *)spmm_tc_kernel<256, __half, false, 1>, (const void *)spmm_tc_kernel<64, float, false, 1>,
+            (const void *)spmm_tc_kernel<128, float, false, 1>, (const void *)spmm_tc_kernel<256, float, false, 1>};
         const void *f8_fns[] = {
             (const void *)spmm_tc_kernel<128, __half, true>, (const void *)spmm_tc_kernel<256, __half, true>,
             (const void *)spmm_tc_kernel<128, float, true>, (const void *)spmm_tc_kernel<256, float, true>,
-            (const void *)spmm_tc_pair_kernel<__half, true>, (const void *)spmm_tc_pair_kernel<float, true>};
+            (const void *)spmm_tc_pair_kernel<__half, true>, (const void *)spmm_tc_pair_kernel<float, true>,
+            (const void *)spmm_tc_kernel<128, __half, true, 1>, (const void *)spmm_tc_kernel<256, __half, true, 1>,
+            (const void *)spmm_tc_kernel<128, float, true, 1>, (const void *)spmm_tc_kernel<256, float, true, 1>};
         int w = 0;
         for (const void *f : f16_fns) {
             if (f8) break;

@@ -120,6 +120,22 @@ def test_plan_bitexact_vs_host_build(cuda, path, sort_rows):
             assert np.array_equal(got, host[key]), f"{name}: {key} differs"
 
 
+@pytest.mark.parametrize("M", [8191, 8192, 8193, 20000])
+@pytest.mark.parametrize("sort_rows", [True, False])
+def test_plan_row_order_both_builders(cuda, M, sort_rows):
+    """Up to 8192 rows the row order (sort, offsets, flags) is built by one
+    block; above, by device-wide sort and scan passes. Both against the host
+    build, bit for bit, with row lengths from 0 to 700 (ties everywhere)."""
+    rng = np.random.default_rng(M)
+    c = gen.small(rng, M, 700, 16, 0.03, empty_rows=0.1)
+    rp, ci, v, _ = dev(c, cuda)
+    plan = tca_spmm.Plan(rp, ci, v, c["K"], sort_rows=sort_rows)
+    host = oracle.build_plan(c["row_ptr"], c["col"], c["vals"], c["K"], sort_rows=sort_rows, path=0)
+    assert plan.info()["n_tc_windows"] == host["n_tc"]
+    for key, which in PLAN_KEYS.items():
+        assert np.array_equal(plan.export(which), host[key]), key
+
+
 @pytest.mark.parametrize("path", ["auto", "tensor_core", "cuda_core"])
 @pytest.mark.parametrize("N", [16, 64, 128, 200, 256, 512])
 @pytest.mark.parametrize("out_dtype", ["f16", "f32"])
