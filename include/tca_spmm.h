@@ -101,7 +101,7 @@ typedef struct tca_plan *tca_plan_t;
 
 typedef struct tca_plan_opts {
     int sort_rows;        /* 1 (default): windows over rows sorted by nnz; 0: natural row order */
-    float tc_min_density; /* windows with condensed density >= this use tensor cores (default 0.02) */
+    float tc_min_density; /* windows with condensed density >= this use tensor cores (default 0.01) */
     int path;             /* 0 auto (default), 1 CUDA cores only, 2 tensor cores only */
     int pair_windows;     /* 0 (default): one tensor-core window per SM; 1: consecutive windows
                              with identical chunk columns run as pairs on two SMs (tcgen05

@@ -172,7 +172,7 @@ def ref_warp_demand(row_ptr, N, warps_per_tb=8) -> np.ndarray:
 
 
 # ---------------------------------------------------------------- tile format
-def build_plan(row_ptr, col_idx, vals, K, sort_rows=True, tc_min_density=0.02, path=0) -> dict:
+def build_plan(row_ptr, col_idx, vals, K, sort_rows=True, tc_min_density=0.01, path=0) -> dict:
     """Host build of the tile format; same arrays as tca_plan_export."""
     L = lib()
     rp, ci, vb = _c(row_ptr, np.int32), _c(col_idx, np.int32), f16_bits(vals)

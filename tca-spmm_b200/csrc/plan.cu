@@ -1145,7 +1145,7 @@ void tca_plan_opts_default(tca_plan_opts_t *o)
     if (!o) return;
     *o = tca_plan_opts_t{};
     o->sort_rows = 1;
-    o->tc_min_density = 0.02f;
+    o->tc_min_density = 0.01f;
     o->path = 0;
     o->pair_windows = 0;
 }

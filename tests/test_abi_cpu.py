@@ -60,7 +60,7 @@ def test_invalid_arguments_rejected_before_device_work():
     assert L.tca_plan_create(None, None, None, -1, 1, 0, None, None, ctypes.byref(h)) == 1
     opts = tca_spmm.PlanOpts()
     L.tca_plan_opts_default(ctypes.byref(opts))
-    assert opts.sort_rows == 1 and opts.path == 0 and abs(opts.tc_min_density - 0.02) < 1e-7
+    assert opts.sort_rows == 1 and opts.path == 0 and abs(opts.tc_min_density - 0.01) < 1e-7
     opts.path = 5
     assert L.tca_plan_create(1, 1, 1, 1, 1, 1, ctypes.byref(opts), None, ctypes.byref(h)) == 1
     # an M == 0 plan needs no device memory and behaves as an empty problem
