@@ -142,6 +142,25 @@ def test_density_threshold_decides_path():
     assert hi["n_tc"] == 0 and lo["n_tc"] == 1
 
 
+def test_default_density_split_of_the_sweep_problem():
+    """The default threshold (0.01) on the 4096 x 1024, 80 % Zipf problem:
+    windows whose rows hold 10 or more nonzeros (16 direct chunks, density
+    >= 0.0126) take the tensor cores, the windows of rows with at most 10 stay
+    on the CUDA cores, among them the windows of one-nonzero
+    rows (128 nonzeros in 2 condensed chunks, density 0.0078)."""
+    c = gen.sweep(0.8, N=256, seed=7000)
+    p = oracle.build_plan(c["row_ptr"], c["col"], c["vals"], c["K"])
+    assert p["n_tc"] == 13 and p["n_cc"] == 19
+    prp = p["p_row_ptr"]
+    for w in p["cc_windows"]:
+        lens = np.diff(prp[w * 128:w * 128 + 129])
+        assert lens.max() <= 10
+    singles = [w for w in p["cc_windows"] if np.all(np.diff(prp[w * 128:w * 128 + 129]) == 1)]
+    assert len(singles) == 12
+    old = oracle.build_plan(c["row_ptr"], c["col"], c["vals"], c["K"], tc_min_density=0.02)
+    assert old["n_tc"] == 11 and set(old["tc_windows"]) < set(p["tc_windows"])
+
+
 def test_malformed_csr_rejected():
     with pytest.raises(ValueError):
         oracle.build_plan(np.array([0, 2, 1], np.int32), np.array([0, 1], np.int32), np.ones(2, np.float16), 4)
