@@ -49,7 +49,7 @@ def cases():
     yield "dense_odd", gen.small(rng, 128 * 7 - 5, 520, 256, 0.08)
     # N not a multiple of 256: the second slice is partly (second half: wholly) outside N
     yield "n320", gen.small(rng, 128 * 6, 256, 320, 0.1)
-    # the sweep problem itself (11 tensor-core windows, 5 pairs + 1 alone)
+    # the sweep problem itself (13 tensor-core windows, 6 pairs + 1 alone)
     yield "sweep80", gen.sweep(0.8, N=256, seed=7000)
 
 
