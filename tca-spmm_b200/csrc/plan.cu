@@ -1051,6 +1051,7 @@ int build_plan(tca_plan *p, const int *row_ptr, const int *col, const __half *va
         put(o_ich, h_img_chunk.data(), sizeof(int) * h_img_chunk.size());
         put(o_cci, cc_items.data(), sizeof(int2) * cc_items.size());
         put(o_alli, all_items.data(), sizeof(int2) * all_items.size());
+        // pageable, as above: h_part may go out of scope when the call returns
         TCA_CUDA_TRY(cudaMemcpyAsync(a, h_part.data(), host_part, cudaMemcpyHostToDevice, s));
     }
     if (p->n_images > 0) {
