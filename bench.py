@@ -151,21 +151,40 @@ def problem_bytes(c, N, c_bytes=2):
     return nnz * (2 + 4) + (c["M"] + 1) * 4 + c["K"] * N * 2 + c["M"] * N * c_bytes
 
 
+def cpu_model():
+    """The host CPU's model name (Linux /proc/cpuinfo), or the platform string."""
+    try:
+        for line in pathlib.Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or platform.machine()
+
+
 def cpu_baseline(c, seconds):
+    """The oracle's OpenMP FP32 CSR x dense SpMM on every host core this
+    process may run on: one warm-up run, then runs until `seconds` have passed
+    (at least 10, at most 1000); the figure is the median run."""
     from oracle import oracle
     nthreads = len(os.sched_getaffinity(0))
     flops = 2.0 * c["col"].size * c["B"].shape[1]
     oracle.spmm_f32(c["row_ptr"], c["col"], c["vals"], c["B"], nthreads=nthreads)  # warm-up
-    reps, t0 = 0, time.perf_counter()
+    times, t_start = [], time.perf_counter()
     while True:
+        t0 = time.perf_counter()
         oracle.spmm_f32(c["row_ptr"], c["col"], c["vals"], c["B"], nthreads=nthreads)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el >= seconds or reps >= 1000:
+        times.append(time.perf_counter() - t0)
+        el = time.perf_counter() - t_start
+        if (el >= seconds and len(times) >= 10) or len(times) >= 1000:
             break
-    return {"value": round(flops * reps / el / 1e9, 3), "unit": "GFLOP/s", "cores": nthreads, "kind": "port",
-            "sample": f"{reps} runs of one {c['M']}x{c['K']} problem (nnz={c['col'].size}, N={c['B'].shape[1]}) "
-                      f"in {el:.1f} s, OpenMP FP32 CSR x dense (oracle/tca_oracle.c orc_spmm_f32)"}
+    med = statistics.median(times)
+    return {"value": round(flops / med / 1e9, 3), "unit": "GFLOP/s", "cores": nthreads, "kind": "port",
+            "cpu_model": cpu_model(),
+            "sample": f"median of {len(times)} runs of one {c['M']}x{c['K']} problem (nnz={c['col'].size}, "
+                      f"N={c['B'].shape[1]}) in {el:.1f} s after one warm-up, OpenMP FP32 CSR x dense "
+                      f"(oracle/tca_oracle.c orc_spmm_f32)"}
 
 
 def dist_setup(args):
@@ -768,7 +787,7 @@ def run_reference(args, world, rank):
         "reference_impl": "naive_gemm (the reference's CPU implementation of the product) from the unmodified "
                           "reference sources in oracle/_ref/libtcaref.so, on the host cores",
         "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": cores, "kind": "reference",
-                         "sample": sample},
+                         "cpu_model": cpu_model(), "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_gpu": {
             "value": round(gpu_value, 3), "unit": "GFLOP/s", "problems": len(distinct),
