@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-per-problem", action="store_true", help="skip the per-problem comparison leg")
-    ap.add_argument("--only", choices=["step", "step_e4m3", "fwd_bwd", "batching", "e2e"], default=None,
+    ap.add_argument("--only", choices=["step", "step_e4m3", "fwd_bwd", "batching", "e2e", "csr", "f64", "cc_mma",
+                                       "pair"], default=None,
                     help="run only this leg (for profiling: ncu captures of one kernel); prints its own line")
     return ap.parse_args()
 
@@ -395,7 +396,10 @@ def run_ours(args, world, rank):
 def run_only(args, world):
     """One leg alone, for profiling runs: the headline step (FP16 or E4M3)
     replayed `steps` times after `warmup`, the differentiation config, the
-    batching config, or the host-buffer forward."""
+    batching config, or the host-buffer forward; or one of the kernels off
+    the headline path on the headline problem: the plan-free forward (csr),
+    the FP64 forward (f64), the step with the CUDA-core rows as mma.sync items
+    (cc_mma) or with window pairs on CTA pairs (pair)."""
     import torch
     import tca_spmm
     if args.only == "fwd_bwd":
@@ -411,14 +415,31 @@ def run_only(args, world):
                                C=np.empty((c["M"], args.n), np.float16), keep_empty_rows=False)
         return {"s": time.perf_counter() - t0}
     dev = torch.device("cuda", torch.cuda.current_device())
+    if args.only in ("csr", "f64"):
+        c = distinct[0]
+        rp, ci = (torch.from_numpy(c[k]).to(dev) for k in ("row_ptr", "col"))
+        if args.only == "csr":
+            v, B = (torch.from_numpy(c[k]).to(dev) for k in ("vals", "B"))
+            C = torch.empty((c["M"], args.n), dtype=torch.float16, device=dev)
+            fn = lambda: tca_spmm.spmm_csr(rp, ci, v, B, K=c["K"], out=C)  # noqa: E731
+        else:
+            v = torch.from_numpy(c["vals"].astype(np.float64)).to(dev)
+            B = torch.from_numpy(c["B"].astype(np.float64)).to(dev)
+            C = torch.empty((c["M"], args.n), dtype=torch.float64, device=dev)
+            fn = lambda: tca_spmm.spmm_csr_f64(rp, ci, v, B, K=c["K"], out=C)  # noqa: E731
+        for _ in range(args.warmup + args.steps):
+            fn()
+        torch.cuda.synchronize()
+        return {"problems": 1}
     plans, Bs, Cs = [], [], []
     for g in range(args.problems):
         c = distinct[g % len(distinct)]
         rp, ci, v, B = (torch.from_numpy(c[k]).to(dev) for k in ("row_ptr", "col", "vals", "B"))
-        plans.append(tca_spmm.Plan(rp, ci, v, c["K"]))
+        plans.append(tca_spmm.Plan(rp, ci, v, c["K"], pair_windows=args.only == "pair"))
         Bs.append(B)
         Cs.append(torch.empty((c["M"], args.n), dtype=torch.float16, device=dev))
-    g = tca_spmm.BatchGraph(plans, Bs, Cs, precision="e4m3" if args.only == "step_e4m3" else "f16")
+    g = tca_spmm.BatchGraph(plans, Bs, Cs, precision="e4m3" if args.only == "step_e4m3" else "f16",
+                            cc_cols=[tca_spmm.CC_COLS_MMA] * len(plans) if args.only == "cc_mma" else None)
     for _ in range(args.warmup + args.steps):
         g.launch()
     torch.cuda.synchronize()
